@@ -1,0 +1,241 @@
+// orc_golden.cpp — TEST INFRASTRUCTURE (the CPU oracle), not product code.
+//
+// Runs the shared per-point restatement (include/koral/*.h) on the input side
+// of the reference's per-function golden records (KGLD, produced by
+// koral-zig's oracle/harness_*.c from C KORAL) and writes the outputs in the
+// record's own output layout, so the tests compare them with the reference
+// tolerances of koral/tests/golden/*_golden_tests.zig. Only tests/ loads this.
+#include <string.h>
+
+#include "../include/koral/kparams.h"
+
+using namespace kp;
+
+namespace {
+
+// koral/testing/golden.zig:226 (sym10) + :241 (geomFromRecord)
+void geom_from_record(const double* v, int len, Geom& g) {
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 5; ++j) {
+      g.gg[i][j] = 0.0;
+      g.GG[i][j] = 0.0;
+    }
+  int n = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) {
+      g.gg[i][j] = v[n];
+      g.gg[j][i] = v[n];
+      g.GG[i][j] = v[10 + n];
+      g.GG[j][i] = v[10 + n];
+      ++n;
+    }
+  g.gdet = (len >= 23) ? v[20] : 1.0;
+  g.gttpert = (len >= 23) ? v[22] : 0.0;
+  g.alpha = (len >= 23) ? v[21] : kmath::sqrt(-1.0 / g.GG[0][0]);
+  for (int i = 0; i < 4; ++i) g.xx[i] = 0.0;
+}
+
+const double kGam = 5.0 / 3.0;
+
+}  // namespace
+
+extern "C" int orc_golden(const char* name, long nrec, const double* in, int nin, double* out, int nout) {
+  const FloorParams fl = floor_params_puffy();
+  const RadParams rp = rad_params_puffy();
+  const OpacParams op = opac_params_puffy(10.0);
+  const ImplicitParams ip = implicit_params_puffy();
+  for (long r = 0; r < nrec; ++r) {
+    const double* a = in + r * nin;
+    double* o = out + r * nout;
+    Geom g;
+    if (!strcmp(name, "p2u")) {
+      geom_from_record(a, 23, g);
+      double uu[NV];
+      p2u(a + 23, uu, g, kGam);
+      for (int i = 0; i < NV; ++i) o[i] = uu[i];
+    } else if (!strcmp(name, "u2p_solver")) {
+      geom_from_record(a, 23, g);
+      double pp[NV];
+      for (int i = 0; i < NV; ++i) pp[i] = a[36 + i];
+      o[0] = u2p_solver_w(a + 23, pp, g, ETYPE_HOT, kGam);
+      for (int i = 0; i < 9; ++i) o[1 + i] = pp[i];
+      for (int i = 0; i < NV; ++i) pp[i] = a[36 + i];
+      o[10] = u2p_solver_w(a + 23, pp, g, ETYPE_ENTROPY, kGam);
+      for (int i = 0; i < 9; ++i) o[11 + i] = pp[i];
+    } else if (!strcmp(name, "floors")) {
+      geom_from_record(a, 23, g);
+      double pp[NV];
+      for (int i = 0; i < NV; ++i) pp[i] = a[23 + i];
+      int guards = 0;
+      o[0] = check_floors_mhd(pp, g, kGam, fl, guards);
+      for (int i = 0; i < NV; ++i) o[1 + i] = pp[i];
+    } else if (!strcmp(name, "physics_tij")) {
+      geom_from_record(a, 20, g);
+      const double* pp = a + 20;
+      double t[4][4], ucon[4], ucov[4], bcon[4], bcov[4], bsq;
+      calc_tij(pp, g, kGam, t);
+      ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], g, ucon, ucov);
+      double B[3] = {pp[B1], pp[B2], pp[B3]};
+      bcon_bcov_bsq(B, ucon, ucov, g, bcon, bcov, bsq);
+      int n = 0;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) o[n++] = t[i][j];
+      for (int i = 0; i < 4; ++i) o[n++] = ucon[i];
+      for (int i = 0; i < 4; ++i) o[n++] = ucov[i];
+      for (int i = 0; i < 4; ++i) o[n++] = bcon[i];
+      for (int i = 0; i < 4; ++i) o[n++] = bcov[i];
+      o[n++] = bsq;
+    } else if (!strcmp(name, "relele_convvels")) {
+      geom_from_record(a, 20, g);
+      double uin[4] = {0.0, a[22], a[23], a[24]}, uo[4] = {0, 0, 0, 0};
+      int e = convert(uin, (int)a[20], (int)a[21], g, RECOMPUTE_UT, uo);
+      for (int i = 0; i < 4; ++i) o[i] = e ? kmath::nan() : uo[i];
+    } else if (!strcmp(name, "relele_boost")) {
+      geom_from_record(a, 20, g);
+      double l[4][4], b1[4], b2[4];
+      lorentz_lab2ff(a[20], a[21], a[22], g, l);
+      boost2_lab2ff(a + 23, a[20], a[21], a[22], g, b1);
+      boost2_ff2lab(a + 23, a[20], a[21], a[22], g, b2);
+      int n = 0;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) o[n++] = l[i][j];
+      for (int i = 0; i < 4; ++i) o[n++] = b1[i];
+      for (int i = 0; i < 4; ++i) o[n++] = b2[i];
+    } else if (!strcmp(name, "recon")) {
+      int param = (int)a[10];
+      int scheme = 2 - param;
+      if (scheme < 0) scheme = 0;
+      Faces f = reconstruct(scheme, a, a + 5, a[11]);
+      o[0] = f.left;
+      o[1] = f.right;
+    } else if (!strcmp(name, "wavespeed")) {
+      geom_from_record(a, 23, g);
+      bool act[3] = {true, true, false};
+      double aa[6];
+      gas_wavespeeds_lr(a + 23, g, kGam, act, aa);
+      for (int i = 0; i < 4; ++i) o[i] = aa[i];
+    } else if (!strcmp(name, "fluxprime")) {
+      geom_from_record(a, 23, g);
+      double ff[NV];
+      int e = f_flux_prime(a + 24, (int)a[23], g, kGam, ff);
+      for (int i = 0; i < NV; ++i) o[i] = e ? kmath::nan() : ff[i];
+    } else if (!strcmp(name, "rad_rij")) {
+      geom_from_record(a, 20, g);
+      double rij[4][4], ucon[4];
+      calc_rij(a + 20, g, rij);
+      double rtt = calc_ff_rtt(a + 20, g, ucon);
+      int n = 0;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) o[n++] = rij[i][j];
+      o[n++] = rtt;
+      for (int i = 0; i < 4; ++i) o[n++] = ucon[i];
+    } else if (!strcmp(name, "rad_u2prad")) {
+      geom_from_record(a, 23, g);
+      double uu[NV], pp[NV];
+      for (int i = 0; i < NV; ++i) {
+        uu[i] = 0.0;
+        pp[i] = 0.0;
+      }
+      for (int i = 0; i < 4; ++i) {
+        uu[EE + i] = a[23 + i];
+        pp[EE + i] = a[27 + i];
+      }
+      U2pRadRes res = u2p_rad(uu, pp, g, rp);
+      o[0] = res.ret;
+      o[1] = res.corrected ? 1.0 : 0.0;
+      for (int i = 0; i < 4; ++i) o[2 + i] = pp[EE + i];
+    } else if (!strcmp(name, "rad_wavespeeds")) {
+      geom_from_record(a, 20, g);
+      bool act[3] = {true, true, false};
+      double aval[12];
+      rad_wavespeeds(a + 20, g, a + 33, act, aval);
+      o[0] = aval[0];
+      o[1] = aval[1];
+      o[2] = aval[2];
+      o[3] = aval[3];
+      o[4] = aval[6];
+      o[5] = aval[7];
+      o[6] = aval[8];
+      o[7] = aval[9];
+    } else if (!strcmp(name, "rad_floors")) {
+      geom_from_record(a, 23, g);
+      double pp[NV];
+      for (int i = 0; i < NV; ++i) pp[i] = a[23 + i];
+      o[0] = check_floors_rad(pp, g, rp);
+      for (int i = 0; i < NV; ++i) o[1 + i] = pp[i];
+    } else if (!strcmp(name, "rad_thermo")) {
+      geom_from_record(a, 23, g);
+      RadState st;
+      fill_rad_state(a + 23, g, kGam, op, true, st);
+      o[0] = st.tgas;
+      o[1] = st.te;
+      o[2] = st.ne;
+      o[3] = st.ehat;
+      o[4] = st.tradbb;
+      o[5] = st.kappaes;
+      o[6] = st.opac.gas_abs;
+      o[7] = st.opac.rad_abs;
+      o[8] = st.opac.gas_num;
+      o[9] = st.opac.rad_num;
+      o[10] = st.opac.gas_ross;
+      o[11] = st.opac.rad_ross;
+      o[12] = st.kappa;
+    } else if (!strcmp(name, "rad_opac")) {
+      geom_from_record(a, 23, g);
+      RadState st;
+      fill_rad_state(a + 23, g, kGam, op, true, st);
+      double kes = calc_kappaes_standalone(a + 23, kGam, op);
+      o[0] = st.kappa;
+      o[1] = kes;
+      o[2] = st.kappa + kes;
+    } else if (!strcmp(name, "rad_gi")) {
+      geom_from_record(a, 23, g);
+      const double* pp = a + 23;
+      RadState st;
+      fill_rad_state(pp, g, kGam, op, true, st);
+      double giff[4], gilab[4];
+      calc_gi_from_state(st, pp[VX], pp[VY], pp[VZ], g, op, true, giff, gilab);
+      for (int i = 0; i < 4; ++i) {
+        o[i] = gilab[i];
+        o[4 + i] = giff[i];
+      }
+      // the test's force scale (koral/tests/golden/opac_golden_tests.zig:108)
+      RadState sens = st;
+      sens.trad = 2.0 * st.te;
+      double b = op.c.sigma_rad_over_pi * st.te * st.te * st.te * st.te;
+      if (nout > 8)
+        o[8] = (st.opac.rad_ross + st.kappaes) * st.ehat + st.opac.gas_abs * op.c.fourpi * b +
+               kmath::fabs(compton_gi_coeff(op.c, sens));
+    } else if (!strcmp(name, "rad_implicit")) {
+      geom_from_record(a, 23, g);
+      double dt = a[23];
+      double pp[NV], uu[NV];
+      for (int i = 0; i < NV; ++i) pp[i] = a[24 + i];
+      ImplicitResult res = solve_implicit_lab(uu, pp, g, dt, kGam, rp, op, ip);
+      o[0] = res.ok ? 0.0 : -1.0;
+      o[1] = res.whichprim;
+      o[2] = res.whicheq;
+      o[3] = res.whichframe;
+      o[4] = res.iters;
+      for (int i = 0; i < NV; ++i) o[5 + i] = pp[i];
+      if (nout > 18) o[18] = res.rung;
+    } else if (!strcmp(name, "implicit_resid")) {
+      // in: geom23 dt pp00[13] cand[13] prim eq frame -> err
+      // (koral/tests/golden/implicit_golden_tests.zig:33 trueResidual)
+      geom_from_record(a, 23, g);
+      double dt = a[23];
+      const double* pp00 = a + 24;
+      const double* cand = a + 37;
+      double uu00[NV], uux[NV], f[4];
+      RadState st00, stx;
+      p2u(pp00, uu00, g, kGam);
+      fill_rad_state(pp00, g, kGam, op, true, st00);
+      p2u(cand, uux, g, kGam);
+      fill_rad_state(cand, g, kGam, op, true, stx);
+      o[0] = implicit_residual(uux, cand, stx, uu00, st00, dt, g, op, (int)a[50], (int)a[51], (int)a[52], f);
+    } else {
+      return -1;
+    }
+  }
+  return 0;
+}

@@ -1,0 +1,102 @@
+"""Convert the reference's committed golden files into the compact .npz
+fixtures the tests read.
+
+The reference (koral-zig) keeps three golden families for the step path:
+  * KGLD  — per-function C-oracle records (koral/testing/golden.zig:32):
+            "KGLD" u32 version, u64 nrec, u32 nin, u32 nout, f64 data[]
+  * KSTP  — forced-dt full-step records of C KORAL (golden.zig:58), optionally
+            gzipped: "KSTP" u32 version, u32 nx,ny,nz,nv, u64 nrec, then per
+            record {t, dt, u[ncell*nv], p[ncell*nv], flags[nf*ncell]}
+  * KSLF  — Zig self-goldens (koral/testing/selfgolden.zig:20), gzipped.
+
+This script is run once where the reference tree is available; its outputs
+under tests/golden/ are what the test suite (and the GPU box) reads.
+
+    python tests/golden/make_fixtures.py /path/to/koral-zig
+"""
+import gzip
+import os
+import struct
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+KGLD = [
+    "state/p2u.kgld", "state/u2p_solver.kgld", "state/floors.kgld", "state/physics_tij.kgld",
+    "state/relele_convvels.kgld", "state/relele_boost.kgld", "state/frames_transpall.kgld",
+    "flux/recon.kgld", "flux/wavespeed.kgld", "flux/fluxprime.kgld", "flux/ct.kgld", "flux/bfroma.kgld",
+    "rad/rad_rij.kgld", "rad/rad_u2prad.kgld", "rad/rad_wavespeeds.kgld", "rad/rad_floors.kgld",
+    "rad/rad_thermo.kgld", "rad/rad_opac.kgld", "rad/rad_gi.kgld", "rad/rad_implicit.kgld",
+    "metric/metric_points.kgld", "metric/coco_dxdx.kgld", "metric/krzysie_grid.kgld",
+]
+KSLF = ["puffy_fast.kslf", "puffy_full.kslf"]
+KSTP = ["step/puffy64.kstp.gz"]
+
+
+def read_maybe_gz(path):
+    raw = open(path, "rb").read()
+    if raw[:2] == b"\x1f\x8b":
+        raw = gzip.decompress(raw)
+    return raw
+
+
+def conv_kgld(src, dst):
+    raw = open(src, "rb").read()
+    assert raw[:4] == b"KGLD" and struct.unpack("<I", raw[4:8])[0] == 1
+    nrec = struct.unpack("<Q", raw[8:16])[0]
+    nin, nout = struct.unpack("<II", raw[16:24])
+    data = np.frombuffer(raw[24:], dtype="<f8").reshape(nrec, nin + nout)
+    np.savez_compressed(dst, nin=nin, nout=nout, data=data)
+
+
+def conv_kslf(src, dst):
+    raw = read_maybe_gz(src)
+    assert raw[:4] == b"KSLF"
+    version, nx, ny, nz, ng, nv = struct.unpack("<IIIIII", raw[4:28])
+    (ncell,) = struct.unpack("<Q", raw[28:36])
+    nflags, nsc, nfield, llen = struct.unpack("<IIII", raw[36:52])
+    off = 52 + llen
+    off += (8 - off % 8) % 8
+    vals = np.frombuffer(raw[off:], dtype="<f8")
+    nscv = nsc * 7
+    scalars = vals[:nscv].reshape(nsc, 7)
+    steps = vals[nscv:nscv + nfield]
+    fl = vals[nscv + nfield:].reshape(nfield, -1)
+    nu = ncell * nv
+    u = fl[:, :nu].reshape(nfield, ncell, nv)
+    p = fl[:, nu:2 * nu].reshape(nfield, ncell, nv)
+    flags = fl[:, 2 * nu:].reshape(nfield, ncell, nflags).astype(np.int32)
+    np.savez_compressed(dst, nx=nx, ny=ny, nz=nz, ng=ng, nv=nv, scalars=scalars, steps=steps, u=u, p=p, flags=flags,
+                        label=raw[52:52 + llen].decode())
+
+
+def conv_kstp(src, dst):
+    raw = read_maybe_gz(src)
+    assert raw[:4] == b"KSTP"
+    version, nx, ny, nz, nv = struct.unpack("<IIIII", raw[4:24])
+    (nrec,) = struct.unpack("<Q", raw[24:32])
+    ncell = nx * ny * nz
+    vals = np.frombuffer(raw[32:], dtype="<f8").reshape(nrec, -1)
+    per = vals.shape[1]
+    nf = (per - 2 - 2 * ncell * nv) // ncell
+    nu = ncell * nv
+    np.savez_compressed(dst, nx=nx, ny=ny, nz=nz, nv=nv, t=vals[:, 0], dt=vals[:, 1],
+                        u=vals[:, 2:2 + nu].reshape(nrec, ncell, nv), p=vals[:, 2 + nu:2 + 2 * nu].reshape(nrec, ncell, nv),
+                        flags=vals[:, 2 + 2 * nu:].reshape(nrec, nf, ncell).astype(np.int32))
+
+
+def main(ref):
+    for rel in KGLD:
+        dst = os.path.join(HERE, rel.replace("/", "__").replace(".kgld", ".npz"))
+        conv_kgld(os.path.join(ref, "tests/golden", rel), dst)
+    for rel in KSLF:
+        conv_kslf(os.path.join(ref, "tests/selfgolden", rel), os.path.join(HERE, rel.replace(".kslf", "_kslf.npz")))
+    for rel in KSTP:
+        name = os.path.basename(rel).replace(".kstp.gz", "_kstp.npz")
+        conv_kstp(os.path.join(ref, "tests/golden", rel), os.path.join(HERE, name))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

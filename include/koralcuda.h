@@ -1,0 +1,177 @@
+/* koralcuda.h — the C ABI of libkoralcuda, the sm_100a GR-RMHD + M1 step engine.
+ *
+ * The reference (koral-zig) has no FFI: its step path sits behind the Zig
+ * generic `Sim(cfg)` (koral/sim.zig:93). Each entry point below replaces one
+ * method or field of that type, cited as file:line in koral-zig; a Zig host
+ * binds them with `extern fn`. All structs are POD,
+ * all arrays are caller-owned host memory copied at the call, and no call
+ * aborts: every failure is an int status plus kc_last_error().
+ *
+ * Host array layout is the reference's Field layout (koral/field.zig:1-10):
+ * AoS, variable fastest, signed cell indices including ghosts,
+ *   offset = ((jz*SY + jy)*SX + jx)*NV + iv,  jx = ix + ngx, ...
+ * with NV = 13 (RHO UU VX VY VZ ENTR B1 B2 B3 EE FX FY FZ) and ghosts
+ * collapsed on size-1 dimensions (koral/grid.zig:17). Flags are six int32 per
+ * cell (koral/sim/storage.zig:11): entropy, entropy2, entropy3, hd_fixup,
+ * rad_fixup, radimp_fixup.
+ */
+#ifndef KORALCUDA_H
+#define KORALCUDA_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KC_ABI_VERSION 1
+#define KC_NV 13
+#define KC_NFLAGS 6
+
+/* status codes (the reference's relele.Error set, koral/relele.zig:51, plus
+ * Sim.init's InvalidConfig, koral/sim.zig:319, and the device-side ones) */
+enum {
+  KC_OK = 0,
+  KC_ERR_INVALID_CONFIG = 1,
+  KC_ERR_OOM = 2,
+  KC_ERR_VELOCITY_CONVERSION = 3,
+  KC_ERR_SPACELIKE = 4,
+  KC_ERR_NAN_IN_FLUX = 5,
+  KC_ERR_CUDA = 6,
+  KC_ERR_TIMEOUT = 7,
+  KC_ERR_NO_DEVICE = 8
+};
+
+enum { KC_BC_PERIODIC = 0, KC_BC_COPY = 1, KC_BC_PUFFY = 2 };
+enum { KC_PLAIN_FP64 = 0, KC_MIXED = 1 };
+enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
+enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1 };
+
+/* koral/grid.zig:22 (Grid.init): internal-coordinate extents */
+typedef struct kc_grid {
+  int32_t nx, ny, nz, ng;
+  double minx, maxx, miny, maxy, minz, maxz;
+} kc_grid;
+
+/* Sim.Options (koral/sim.zig:130) as built by the PUFFY problem's
+ * Physics.toOptions (koral/problems/puffy/puffy.zig:210). */
+typedef struct kc_options {
+  int32_t abi_version;
+  /* metric (koral/metric/forms.zig:16) and units (koral/units.zig:37) */
+  double bhspin, mksr0, mksh0, mass;
+  double gam, tsteplim, minmod_theta;
+  /* FloorParams (koral/solve/invert.zig:60) */
+  double rhofloor, uurhoratiomin, uurhoratiomax, b2rhoratiomax, b2uuratiomax, gammamaxhd;
+  int32_t isentropic_b2rhofloors, b2uufloor;
+  double horizon_x1;
+  /* RadParams (koral/solve/invert_rad.zig:36) */
+  double gammamaxrad, eradfloor, eerhoratiomin, eerhoratiomax, eeuuratiomin, eeuuratiomax;
+  /* opacity channels and composition (koral/physics/opacities.zig:61, thermo.zig:33) */
+  int32_t bremsstrahlung, synchrotron, kleinnishina, comptonization, synchrotron_bridge;
+  int32_t scattering; /* Klein-Nishina kappa_es hook on/off (PR_KAPPAES) */
+  double hfrac, hefrac, mu_gas, mu_i, mu_e;
+  /* ImplicitParams (koral/solve/implicit.zig:83) */
+  double radimp_conv, radimp_entrconv, radimp_eps;
+  int32_t radimp_maxiter;
+  double radimp_convrel, radimp_convrelerr, radimp_convrelentr, radimp_convrelentrerr;
+  double radimp_damping_factor, radimp_max_en_change_down, radimp_max_en_change_up, radimp_max_damping;
+  double radimp_max_tgas_change, radimp_max_trad_change, radimp_threshold;
+  int32_t radimp_start_with_bisect, radimp_scale_jacobian, radimp_allow_rad_ceiling, radimp_allow_entr_in_4dprim;
+  int32_t radimp_opdamp_maxlevels;
+  double radimp_opdamp_factor;
+  int32_t radimp_lag_opac;
+  /* fixups, polar axis, radiative viscosity, dynamo (koral/sim.zig:150-180) */
+  int32_t do_fixups, do_u2prad_fixups, do_radimp_fixups;
+  int32_t correct_polaraxis, nccorrectpolar;
+  int32_t radviscosity;
+  double alpharadvisc, maxradviscvel;
+  int32_t dynamo;
+  double alphadynamo, thetaangle, alphabeta, betasaturated, expectedhr;
+  int32_t alphaflipssign, dampbeta, calchronthego;
+  int32_t reduceorderatbh, reduceorderafterfixup, dampradwavespeednearaxis;
+  int32_t bc_x, bc_y, bc_z;
+  /* engine forms (no reference counterpart) */
+  int32_t precision;     /* KC_PLAIN_FP64 | KC_MIXED */
+  int32_t implicit_mode; /* KC_IMPLICIT_PER_CELL | KC_IMPLICIT_COMPACTING */
+  int32_t device;        /* CUDA device ordinal */
+} kc_options;
+
+/* Sim counters and step scalars (koral/sim.zig:237-293, invert.zig:44) */
+typedef struct kc_counters {
+  double t, dt, own_dt, tstepdenmax, tstepdenmin;
+  int64_t nstep;
+  int64_t n_radimp_failures, n_radimp_fail_step, n_radimp_iters, n_radimp_solves;
+  int64_t n_guard_recoveries;
+} kc_counters;
+
+typedef struct kc_step_info {
+  double dt;
+  int64_t nan_cell; /* first flat cell index whose face flux was non-finite, or -1 */
+} kc_step_info;
+
+typedef struct kc_handle kc_handle;
+
+/* Fills the PUFFY option set (puffy.zig:210 toOptions with Physics defaults,
+ * puffy.zig:84). */
+void kc_options_puffy(kc_options* opt);
+/* The PUFFY grid (puffy.zig:179 makeGridNz). */
+void kc_grid_puffy(int32_t nx, int32_t ny, int32_t nz, kc_grid* grid);
+
+/* Sim.init (koral/sim.zig:309): validates, builds the metric cache and
+ * allocates the device state. */
+int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out);
+/* Sim.deinit (koral/sim.zig:501) */
+void kc_destroy(kc_handle* h);
+const char* kc_last_error(const kc_handle* h);
+
+/* Sim.p / Sim.u / Sim.flags field access (koral/sim.zig:224-262) */
+int kc_upload_prims(kc_handle* h, const double* p_aos);
+int kc_upload_cons(kc_handle* h, const double* u_aos);
+int kc_upload_flags(kc_handle* h, const int32_t* flags);
+int kc_download_prims(kc_handle* h, double* p_aos);
+int kc_download_cons(kc_handle* h, double* u_aos);
+int kc_download_flags(kc_handle* h, int32_t* flags);
+/* restores t, dt, tstepdenmax/min and the counters (restart / replay) */
+int kc_set_counters(kc_handle* h, const kc_counters* c);
+int kc_get_counters(kc_handle* h, kc_counters* c);
+
+/* PUFFY initial state: puffy.initAllWith (puffy.zig:873) — limotorus,
+ * atmosphere, A_phi seed, B from A, beta normalization. perturb is the
+ * relative u_int noise amplitude and seed mixes into the per-cell hash
+ * (puffy.zig:696 perturbXi); pass 0 for the unperturbed reference init. */
+int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed);
+/* Sim.finishInit (koral/sim.zig:686): ghost fill from p, then the dt guess */
+int kc_finish_init(kc_handle* h);
+/* Sim.initTimestepGuess (koral/sim.zig:693) */
+int kc_init_timestep_guess(kc_handle* h);
+/* Sim.setBc / Sim.calcU2p (koral/sim.zig:735, :924) */
+int kc_set_bc(kc_handle* h);
+int kc_calc_u2p(kc_handle* h);
+/* Sim.cflDt (koral/sim.zig:726) */
+int kc_cfl_dt(kc_handle* h, double* dt);
+/* Sim.step (koral/sim.zig:1792): forced_dt NaN means the CFL dt. */
+int kc_step(kc_handle* h, double forced_dt, kc_step_info* info);
+/* host buffers -> step(s) -> host buffers in one call */
+int kc_step_n(kc_handle* h, int32_t nsteps, double forced_dt);
+
+/* Engine forms (no reference counterpart) */
+int kc_set_precision(kc_handle* h, int32_t mode);
+int kc_set_implicit_mode(kc_handle* h, int32_t mode);
+int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweights);
+
+/* Batched per-cell entry points over n independent cells (the C4 implicit
+ * microbench and the parity harnesses). geom23 is the reference's golden
+ * record geometry (gg upper triangle, GG upper triangle, gdet, alpha,
+ * gttpert; koral/testing/golden.zig:241). Arrays are host memory, cell-major.
+ * solveImplicitLab (koral/solve/implicit.zig:927): pp is in/out, res is
+ * {ok, rung, iters, whichprim, whicheq, whichframe} per cell. */
+int kc_implicit_batch(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
+                      int32_t* res, int32_t mode);
+/* u2p cascade of one cell as calcU2p applies it (koral/sim.zig:972-994):
+ * u2pMhd + u2pRad + both floors. flags_out: {entropy_used, hd_fixup, rad_fixup} */
+int kc_u2p_batch(const kc_options* opt, int64_t n, const double* geom23, const double* uu, double* pp,
+                 int32_t* flags_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

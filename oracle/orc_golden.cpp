@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include "../include/koral/kparams.h"
+#include "../include/koral/kmetric.h"
 
 using namespace kp;
 
@@ -233,6 +234,50 @@ extern "C" int orc_golden(const char* name, long nrec, const double* in, int nin
       p2u(cand, uux, g, kGam);
       fill_rad_state(cand, g, kGam, op, true, stx);
       o[0] = implicit_residual(uux, cand, stx, uu00, st00, dt, g, op, (int)a[50], (int)a[51], (int)a[52], f);
+    } else if (!strcmp(name, "metric_points")) {
+      // coords, x0..x3 -> gg16 GG16 gdet dlgdet3 Kr64 gttpert
+      int id = (int)a[0];
+      int co = id == 1 ? BL : id == 2 ? KS : id == 4 ? MINK : MKS2;
+      MetricParams mp = {0.0, 0.1, 0.9};
+      CoordData d;
+      metric_compute(co, mp, a + 1, d);
+      int n = 0;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) o[n++] = d.gcov[i][j];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) o[n++] = d.gcon[i][j];
+      o[n++] = d.gdet;
+      for (int i = 0; i < 3; ++i) o[n++] = d.dlgdet[i];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          for (int k = 0; k < 4; ++k) o[n++] = d.kris[i][j][k];
+      o[n++] = d.gttpert;
+    } else if (!strcmp(name, "coco_dxdx")) {
+      auto cid = [](double v) { int id = (int)v; return id == 1 ? BL : id == 2 ? KS : id == 4 ? MINK : MKS2; };
+      MetricParams mp = {0.0, 0.1, 0.9};
+      int from = cid(a[0]), to = cid(a[1]);
+      double y[4], m[4][4];
+      coco_full(a + 2, from, to, mp, y);
+      dxdx(a + 2, from, to, mp, m);
+      for (int i = 0; i < 4; ++i) o[i] = y[i];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) o[4 + i * 4 + j] = m[i][j];
+    } else if (!strcmp(name, "krzysie_grid")) {
+      // PUFFY 384x360 grid (koral/tests/golden/metric_golden_tests.zig:133)
+      MetricParams mp = {0.0, 0.1, 0.9};
+      Grid gr = grid_init(384, 360, 1, 3, kmath::log(1.85 - 0.1), kmath::log(500.0 - 0.1), 0.001, 1.0 - 0.001,
+                          -KP_PI / 4.0, KP_PI / 4.0);
+      long ix = (long)a[0], iy = (long)a[1];
+      o[0] = grid_xc(gr, ix);
+      o[1] = grid_yc(gr, iy);
+      double x[4] = {0.0, grid_xc(gr, ix), grid_yc(gr, iy), grid_zc(gr, 0)};
+      CoordData d;
+      metric_compute(MKS2, mp, x, d);
+      apply_kris_correction(MKS2, mp, gr, d, ix, iy, 0);
+      int n = 2;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          for (int k = 0; k < 4; ++k) o[n++] = d.kris[i][j][k];
     } else {
       return -1;
     }

@@ -53,7 +53,8 @@ class DevTracker:
         c = np.asarray(c, dtype=np.float64)
         z = np.asarray(z, dtype=np.float64)
         dev = np.abs(c - z) / np.maximum(1.0, np.maximum(np.abs(c), np.abs(z)))
-        dev = np.where(np.isnan(dev), np.inf, dev)
+        # a NaN deviation never wins `dev > max_dev` in the reference tracker
+        dev = np.where(np.isnan(dev), 0.0, dev)
         m = float(np.max(dev)) if dev.size else 0.0
         if m > self.max_dev:
             self.max_dev = m

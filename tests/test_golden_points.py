@@ -226,3 +226,40 @@ def test_implicit_rung_ladder():
     assert st["rung_agree"] * 10 >= st["both_ok"] * 9, st
     assert st["compared"] >= 40, st
     assert st["worst"] <= 1e-6, st
+
+
+def test_metric_points():
+    i, o = load_kgld("metric/metric_points")
+    z = run_golden("metric_points", i, 101)
+    mks2 = i[:, 0] == 10
+    t = DevTracker()
+    t.add(o[:, :16], z[:, :16])
+    t.check(1e-13, "gcov")
+    for sl, b_exact, b_mks2, what in [(slice(16, 32), 1e-13, 1e-8, "gcon"), (slice(32, 33), 1e-13, 1e-8, "gdet"),
+                                      (slice(33, 36), 1e-12, 1e-8, "dlgdet"), (slice(36, 100), 1e-12, 1e-8, "kris")]:
+        t = DevTracker()
+        t.add(o[~mks2, sl], z[~mks2, sl])
+        t.check(b_exact, what + " bl/ks/mink")
+        t = DevTracker()
+        t.add(o[mks2, sl], z[mks2, sl])
+        t.check(b_mks2, what + " mks2")
+    t = DevTracker()
+    t.add(o[:, 100], z[:, 100])
+    t.check(1e-13, "gttpert")
+
+
+def test_coco_and_jacobians():
+    i, o = load_kgld("metric/coco_dxdx")
+    z = run_golden("coco_dxdx", i, 20)
+    err = np.abs(o - z) / np.maximum(1.0, np.maximum(np.abs(o), np.abs(z)))
+    assert np.all(err <= 1e-12), float(np.nanmax(err))
+
+
+def test_corrected_christoffels_on_puffy_grid():
+    i, o = load_kgld("metric/krzysie_grid")
+    z = run_golden("krzysie_grid", i, 66)
+    err = np.abs(o[:, :2] - z[:, :2]) / np.maximum(1.0, np.abs(o[:, :2]))
+    assert np.all(err <= 1e-14)
+    t = DevTracker()
+    t.add(o[:, 2:], z[:, 2:])
+    t.check(1e-8, "kris-corrected mks2")

@@ -1,0 +1,60 @@
+"""The CPU oracle's full RK2IMEX step against the reference's Zig self-goldens
+(tests/selfgolden/puffy_{fast,full}.kslf, produced by
+koral/testing/selfscenarios.zig:94 run): the post-init snapshot is loaded,
+the oracle steps with its own CFL dt, and the per-step scalars, the flag maps
+and the final fields are compared.
+
+Bit identity is not expected: the Zig libm (std.math pow/log/exp) is not in
+this tree and the implicit Newton solve exits on relative-change tolerances,
+so last-bit differences in transcendentals move converged values at the
+1e-12..1e-9 level. The bounds below are the measured deviation with margin.
+"""
+import numpy as np
+import pytest
+
+from tests.kgold import GOLDEN
+from tests.orcsim import OracleSim, puffy_grid, puffy_options
+
+FIELDS = ["rho", "uu", "vx", "vy", "vz", "entr", "b1", "b2", "b3", "ee", "fx", "fy", "fz"]
+
+
+def run_scenario(name):
+    z = np.load(f"{GOLDEN}/{name}_kslf.npz")
+    sim = OracleSim(puffy_grid(int(z["nx"]), int(z["ny"])), puffy_options())
+    sc = z["scalars"]
+    sim.set_state(z["p"][0], z["u"][0], z["flags"][0])
+    sim.lib.orc_sim_init_timestep_guess(sim.h)
+    c = sim.counters()
+    assert c["tstepdenmax"] == sc[0, 3]  # initTimestepGuess is exact
+    rows = []
+    for k in range(1, sc.shape[0]):
+        sim.step()
+        c = sim.counters()
+        rows.append((c["t"], c["dt"], c["own_dt"], c["tstepdenmax"], c["tstepdenmin"], c["n_radimp_failures"],
+                     c["n_radimp_iters"]))
+    return z, sim, np.array(rows)
+
+
+def field_scale_dev(a, b):
+    return np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1e-300)
+
+
+@pytest.mark.parametrize("name,steps_bound,rho_bound", [("puffy_fast", 1e-14, 1e-13), ("puffy_full", 1e-13, 1e-13)])
+def test_oracle_tracks_zig_selfgolden(name, steps_bound, rho_bound):
+    z, sim, rows = run_scenario(name)
+    sc = z["scalars"][1:]
+    # dt sequence (the sim's own CFL choice) and t
+    assert np.all(np.abs(rows[:, 1] / sc[:, 1] - 1) < steps_bound), (rows[:, 1], sc[:, 1])
+    assert np.all(np.abs(rows[:, 0] - sc[:, 0]) <= steps_bound * np.abs(sc[:, 0]))
+    # no implicit failures in either, iteration totals within 0.2%
+    assert np.array_equal(rows[:, 5], sc[:, 5])
+    assert np.all(np.abs(rows[:, 6] / sc[:, 6] - 1) < 2e-3)
+    # flag maps identical cell for cell (incl. ghosts)
+    assert np.array_equal(sim.flags(), z["flags"][1])
+    dev = field_scale_dev(sim.prims(), z["p"][1])
+    report = {f: float(d) for f, d in zip(FIELDS, dev)}
+    print(name, report)
+    assert dev[0] < rho_bound
+    for f in ["uu", "vx", "vy", "vz", "entr", "b1", "b2", "b3", "ee", "fz"]:
+        assert report[f] < 1e-8, (f, report[f])
+    assert report["fx"] < 5e-2 and report["fy"] < 5e-2

@@ -1,0 +1,894 @@
+// kc_engine.cu — libkoralcuda: the host side of the sm_100a step engine and
+// its C ABI (include/koralcuda.h). One engine instance owns one CUDA stream
+// and all device state of one Sim; Sim.step (koral/sim.zig:1792) becomes a
+// fixed sequence of kernel launches on that stream with no host round trip
+// until the step's scalars are read back at its end.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "kc_kernels.cuh"
+
+using namespace kp;
+using namespace kc;
+
+namespace {
+
+const int TPB = 128;
+inline unsigned nblk(long n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+template <class Fn>
+void host_par(long lo, long hi, Fn fn) {
+  unsigned nt = std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if (nt > 32) nt = 32;
+  std::vector<std::thread> th;
+  long n = hi - lo;
+  for (unsigned w = 0; w < nt; ++w) {
+    long a = lo + n * w / nt, b = lo + n * (w + 1) / nt;
+    th.emplace_back([=]() {
+      for (long i = a; i < b; ++i) fn(i);
+    });
+  }
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
+
+struct kc_handle {
+  kc_grid kg;
+  kc_options opt;
+  SimParams sp;
+  DGrid gr;
+  DevState ds;
+  DevScalars* dsc = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  // stage buffers (koral/sim.zig:220)
+  double *ut0 = nullptr, *ut1 = nullptr, *ut2 = nullptr, *dut1 = nullptr, *dut2 = nullptr, *drt1 = nullptr,
+         *drt2 = nullptr, *uforget = nullptr, *staging = nullptr;
+  int* flag_staging = nullptr;
+  // step scalars (koral/sim.zig:237-293)
+  double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
+  double min_dx = 0, min_dy = 0, min_dz = 0;
+  long long nstep = 0, n_fail = 0, n_fail_step = 0, n_iters = 0, n_solves = 0, n_guard = 0;
+  std::string err;
+  int last_status = 0;
+};
+
+namespace {
+
+int fail(kc_handle* h, int code, const std::string& msg) {
+  if (h) {
+    h->err = msg;
+    h->last_status = code;
+  }
+  return code;
+}
+int cuda_check(kc_handle* h, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return KC_OK;
+  return fail(h, KC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+template <class T>
+T* dalloc(kc_handle* h, size_t n, int& st) {
+  void* p = nullptr;
+  if (st) return nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    st = fail(h, KC_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  cudaMemset(p, 0, n * sizeof(T) + 16);
+  h->allocs.push_back(p);
+  return (T*)p;
+}
+
+// ---- metric cache, host-built once (koral/metric/precompute.zig:175) ----------
+int build_cache(kc_handle* h) {
+  const Grid& g = h->gr.g;
+  const MetricParams mp = h->sp.mp;
+  long nc = h->gr.nc, sx = h->gr.sx, sy = h->gr.sy, sz = h->gr.sz;
+  std::vector<double> cgc(NGC * nc), cGc(NGCON * nc), kr(NKR * nc), jbl(16 * nc), blg(NBL * nc);
+  long ngh = (long)h->gr.ngx * sy * sz;
+  std::vector<double> jb2m(16 * (ngh > 0 ? ngh : 1), 0.0);
+  std::vector<int> asym(sy * sz, 0);
+  long yr = sy, zr = sz;
+  host_par(0, zr * yr, [&](long k) {
+    long iz = k / yr - g.ngz, iy = k % yr - g.ngy;
+    for (long ix = -g.ngx; ix < g.nx + g.ngx; ++ix) {
+      long c = (ix + g.ngx) + (iy + g.ngy) * sx + (iz + g.ngz) * sx * sy;
+      double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
+      CoordData d;
+      metric_compute(MKS2, mp, x, d);
+      apply_kris_correction(MKS2, mp, g, d, ix, iy, iz);
+      for (int i = 0; i < 4; ++i)
+        for (int j = i; j < 4; ++j) {
+          cgc[(long)sym10(i, j) * nc + c] = d.gcov[i][j];
+          if (memcmp(&d.gcov[i][j], &d.gcov[j][i], 8)) asym[k] = 1;
+        }
+      cgc[10L * nc + c] = d.gdet;
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) cGc[(long)(i * 4 + j) * nc + c] = d.gcon[i][j];
+      cGc[16L * nc + c] = d.gttpert;
+      for (int l = 0; l < 4; ++l)
+        for (int m = 0; m < 4; ++m)
+          for (int n = m; n < 4; ++n) {
+            kr[(long)(l * 10 + sym10(m, n)) * nc + c] = d.kris[l][m][n];
+            if (memcmp(&d.kris[l][m][n], &d.kris[l][n][m], 8)) asym[k] = 1;
+          }
+      double m4[4][4];
+      dxdx(x, MKS2, BL, mp, m4);
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) jbl[(long)(i * 4 + j) * nc + c] = m4[i][j];
+      Geom gb;
+      geometry_bl_at(g, mp, ix, iy, iz, gb);
+      for (int i = 0; i < 4; ++i)
+        for (int j = i; j < 4; ++j) {
+          blg[(long)sym10(i, j) * nc + c] = gb.gg[i][j];
+          if (memcmp(&gb.gg[i][j], &gb.gg[j][i], 8)) asym[k] = 1;
+        }
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) blg[(long)(10 + i * 4 + j) * nc + c] = gb.GG[i][j];
+      blg[26L * nc + c] = gb.xx[1];
+      blg[27L * nc + c] = gb.xx[2];
+      if (ix >= g.nx) {
+        long gi = (ix - g.nx) + (long)g.ngx * ((iy + g.ngy) + sy * (iz + g.ngz));
+        double xbl[4] = {0.0, gb.xx[1], gb.xx[2], gb.xx[3]};
+        dxdx(xbl, BL, MKS2, mp, m4);
+        for (int i = 0; i < 4; ++i)
+          for (int j = 0; j < 4; ++j) jb2m[(long)(i * 4 + j) * ngh + gi] = m4[i][j];
+      }
+    }
+  });
+  for (int a : asym)
+    if (a) return fail(h, KC_ERR_INVALID_CONFIG, "metric cache is not bitwise symmetric where the packed layout needs it");
+  std::vector<double> fgc[3], fGc[3];
+  for (int dim = 0; dim < 3; ++dim) {
+    long nf = h->ds.nf[dim];
+    fgc[dim].assign(NGC * nf, 0.0);
+    fGc[dim].assign(NGCON * nf, 0.0);
+  }
+  long yr1 = sy + 1, zr1 = sz + 1;
+  auto put = [&](int dim, long f, const CoordData& d) {
+    long nf = h->ds.nf[dim];
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) fgc[dim][(long)sym10(i, j) * nf + f] = d.gcov[i][j];
+    fgc[dim][10L * nf + f] = d.gdet;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) fGc[dim][(long)(i * 4 + j) * nf + f] = d.gcon[i][j];
+    fGc[dim][16L * nf + f] = d.gttpert;
+  };
+  host_par(0, zr1 * yr1, [&](long k) {
+    long iz = k / yr1 - g.ngz, iy = k % yr1 - g.ngy;
+    long nxh = g.nx + g.ngx, nyh = g.ny + g.ngy, nzh = g.nz + g.ngz;
+    for (long ix = -g.ngx; ix <= nxh; ++ix) {
+      long jx = ix + g.ngx, jy = iy + g.ngy, jz = iz + g.ngz;
+      CoordData d;
+      if (iy < nyh && iz < nzh) {
+        double x[4] = {0.0, grid_xl(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
+        metric_compute(MKS2, mp, x, d);
+        put(0, jx + jy * (sx + 1) + jz * sy * (sx + 1), d);
+      }
+      if (ix < nxh && iz < nzh) {
+        double x[4] = {0.0, grid_xc(g, ix), grid_yl(g, iy), grid_zc(g, iz)};
+        metric_compute(MKS2, mp, x, d);
+        put(1, jx + jy * sx + jz * (sy + 1) * sx, d);
+      }
+      if (ix < nxh && iy < nyh) {
+        double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zl(g, iz)};
+        metric_compute(MKS2, mp, x, d);
+        put(2, jx + jy * sx + jz * sy * sx, d);
+      }
+    }
+  });
+  int st = 0;
+  auto up = [&](const std::vector<double>& v) -> const double* {
+    double* p = dalloc<double>(h, v.size(), st);
+    if (p) cudaMemcpy(p, v.data(), v.size() * 8, cudaMemcpyHostToDevice);
+    return p;
+  };
+  h->ds.cgc = up(cgc);
+  h->ds.cGc = up(cGc);
+  h->ds.kr = up(kr);
+  h->ds.jbl = up(jbl);
+  h->ds.blg = up(blg);
+  h->ds.jb2m = up(jb2m);
+  for (int dim = 0; dim < 3; ++dim) {
+    h->ds.fgc[dim] = up(fgc[dim]);
+    h->ds.fGc[dim] = up(fGc[dim]);
+  }
+  return st;
+}
+
+// ---- pass wrappers (one launch each) -----------------------------------------
+int sync_check(kc_handle* h, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_check(h, e, what);
+  return KC_OK;
+}
+
+BcArgs bc_args(kc_handle* h) {
+  BcArgs a;
+  a.bc[0] = h->sp.bc[0];
+  a.bc[1] = h->sp.bc[1];
+  a.bc[2] = h->sp.bc[2];
+  a.gam = h->sp.gam;
+  return a;
+}
+
+// C set_bc (koral/sim/bc.zig:40)
+void launch_set_bc(kc_handle* h) {
+  const DGrid& gr = h->gr;
+  BcArgs a = bc_args(h);
+  cudaStream_t st = h->stream;
+  if (gr.ngx > 0) k_bc_faces<<<nblk(2L * gr.ngx * gr.ny * gr.nz), TPB, 0, st>>>(h->ds, h->dsc, a, 0);
+  if (gr.ngy > 0) k_bc_faces<<<nblk(2L * gr.ngy * gr.nx * gr.nz), TPB, 0, st>>>(h->ds, h->dsc, a, 1);
+  if (gr.ngz > 0) k_bc_faces<<<nblk(2L * gr.ngz * gr.nx * gr.ny), TPB, 0, st>>>(h->ds, h->dsc, a, 2);
+  if (gr.ny > 1 && gr.nz == 1) {
+    k_corners_2d<<<1, 32, 0, st>>>(h->ds, a);
+  } else if (gr.nz > 1 && gr.ny > 1) {
+    long ng = gr.ng;
+    k_edge_tubes<<<nblk(4L * (gr.nz + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 0, 1, 2);
+    k_edge_tubes<<<nblk(4L * (gr.ny + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 0, 2, 1);
+    k_edge_tubes<<<nblk(4L * (gr.nx + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 1, 2, 0);
+    k_corner_cubes<<<nblk(ng * ng * ng), TPB, 0, st>>>(h->ds, a.gam);
+  }
+}
+
+void launch_calc_u2p(kc_handle* h) {
+  const DGrid& gr = h->gr;
+  long ndom = (long)gr.nx * gr.ny * gr.nz;
+  int pnc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
+  cudaMemsetAsync(&h->dsc->any_hd, 0, sizeof(int), h->stream);
+  k_u2p<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, h->sp.fl, h->sp.rp, pnc);
+  if (h->sp.do_fixups) {
+    k_fixup_hd<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, pnc);
+    k_fixup_apply<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc);
+  }
+  launch_set_bc(h);
+}
+
+void launch_do_correct(kc_handle* h) {
+  if (!h->sp.correct_polaraxis) return;
+  const DGrid& gr = h->gr;
+  int ncp = h->sp.nccorrectpolar;
+  k_polar_correct<<<nblk((long)gr.nx * gr.nz * 2 * ncp), TPB, 0, h->stream>>>(h->ds, h->sp.gam, ncp);
+}
+
+void launch_implicit(kc_handle* h, double dtin) {
+  const DGrid& gr = h->gr;
+  ImplArgs a;
+  a.gam = h->sp.gam;
+  a.dt = dtin;
+  a.rp = h->sp.rp;
+  a.op = h->sp.op;
+  a.ip = h->sp.ip;
+  a.polar_nc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
+  k_implicit<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
+}
+
+void launch_wavespeeds(kc_handle* h) {
+  const DGrid& gr = h->gr;
+  WsArgs a;
+  a.gam = h->sp.gam;
+  a.tsteplim = h->sp.tsteplim;
+  a.op = h->sp.op;
+  a.damp_nc = h->sp.dampradwavespeednearaxis;
+  long n = (long)(gr.nx + 2 * (gr.nx > 1)) * (gr.ny + 2 * (gr.ny > 1)) * (gr.nz + 2 * (gr.nz > 1));
+  k_wavespeeds<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
+}
+
+void launch_face_fluxes(kc_handle* h) {
+  const DGrid& gr = h->gr;
+  FluxArgs a;
+  a.gam = h->sp.gam;
+  a.theta = h->sp.minmod_theta;
+  a.maxvel = h->sp.maxradviscvel;
+  a.fl = h->sp.fl;
+  a.radvisc = h->sp.radviscosity;
+  long dims[3] = {gr.nx, gr.ny, gr.nz};
+  for (int d = 0; d < 3; ++d) cudaMemsetAsync(h->ds.flb[d], 0, (size_t)NV * h->ds.nf[d] * 8, h->stream);
+  for (int dim = 0; dim < 3; ++dim) {
+    if (dims[dim] <= 1) continue;
+    int c0 = dim == 0 ? 1 : 0, c1 = dim == 2 ? 1 : 2;
+    long n0 = dims[c0] > 1 ? dims[c0] + 2 : dims[c0];
+    long n1 = dims[c1] > 1 ? dims[c1] + 2 : dims[c1];
+    long n = (dims[dim] + 1) * n0 * n1;
+    k_face_flux<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
+  }
+}
+
+void launch_flux_ct(kc_handle* h) {
+  const DGrid& gr = h->gr;
+  long n = (long)(gr.nx + 1) * (gr.ny + 1) * (gr.nz + 1);
+  k_ct_emf<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  k_ct_rebuild<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+}
+
+void launch_op_explicit(kc_handle* h, double dtin) {
+  launch_wavespeeds(h);
+  launch_face_fluxes(h);
+  launch_flux_ct(h);
+  const DGrid& gr = h->gr;
+  k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dtin);
+  launch_calc_u2p(h);
+}
+
+void launch_rijvisc(kc_handle* h, double global_dt) {
+  const DGrid& gr = h->gr;
+  cudaMemsetAsync(h->ds.rijvisc, 0, (size_t)16 * gr.nc * 8, h->stream);
+  ViscArgs a;
+  a.gam = h->sp.gam;
+  a.dt = global_dt;
+  a.rhor = r_horizon_bl(h->sp.mp.a);
+  a.alpha = h->sp.alpharadvisc;
+  a.op = h->sp.op;
+  long n = (long)(gr.nx + 2 * (gr.nx > 1)) * (gr.ny + 2 * (gr.ny > 1)) * (gr.nz + 2 * (gr.nz > 1));
+  k_rijvisc<<<nblk(n), TPB, 0, h->stream>>>(h->ds, a);
+}
+
+void launch_dynamo(kc_handle* h, double dt) {
+  const DGrid& gr = h->gr;
+  k_scale_height<<<nblk(gr.nx, 64), 64, 0, h->stream>>>(h->ds);
+  launch_set_bc(h);
+  DynArgs a;
+  a.gam = h->sp.gam;
+  a.dt = dt;
+  a.a = h->sp.mp.a;
+  a.rhor = r_horizon_bl(h->sp.mp.a);
+  a.risco = r_isco_bl(h->sp.mp.a);
+  a.dp = h->sp.dp;
+  long n = (long)(gr.nx + 2 * (gr.nx > 1)) * (gr.ny + 2 * (gr.ny > 1)) * (gr.nz + 2 * (gr.nz > 1));
+  k_dynamo_delta_a<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
+  long my = gr.ny == 1 ? 1 : gr.ny + 1, mz = gr.nz == 1 ? 1 : gr.nz + 1;
+  k_corner_avg_a<<<nblk((long)(gr.nx + 1) * my * mz, 256), 256, 0, h->stream>>>(h->ds, h->ds.dyn_a, 1);
+  k_curl_apply<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, 0);
+  launch_calc_u2p(h);
+}
+
+void launch_stage_deriv(kc_handle* h, double* dst, const double* a, const double* b, double delta) {
+  const DGrid& gr = h->gr;
+  k_stage_deriv<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds, dst, a, b, delta);
+}
+void launch_stage_combine(kc_handle* h, double* dst, const double* a, double f1, const double* b, double f2,
+                          const double* c) {
+  const DGrid& gr = h->gr;
+  k_stage_combine<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds, dst, a, f1, b, f2, c);
+}
+void copy_field(kc_handle* h, double* dst, const double* src) {
+  cudaMemcpyAsync(dst, src, (size_t)NV * h->gr.nc * 8, cudaMemcpyDeviceToDevice, h->stream);
+}
+
+void reset_step_scalars(kc_handle* h) {
+  DevScalars z;
+  memset(&z, 0, sizeof(z));
+  double big = 1.0e50;
+  memcpy(&z.tsd_min_bits, &big, 8);
+  cudaMemcpyAsync(h->dsc, &z, sizeof(z), cudaMemcpyHostToDevice, h->stream);
+}
+
+// read the device scalars, fold them into the handle (sim.zig:634 reduceStepGlobals)
+int collect_step_scalars(kc_handle* h, bool fold_cfl) {
+  DevScalars z;
+  cudaError_t e = cudaMemcpyAsync(&z, h->dsc, sizeof(z), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_check(h, e, "step");
+  if (fold_cfl) {
+    if (z.tsd_max_bits) {
+      double m;
+      memcpy(&m, &z.tsd_max_bits, 8);
+      if (m > h->tstepdenmax) h->tstepdenmax = m;
+    }
+    double n;
+    memcpy(&n, &z.tsd_min_bits, 8);
+    if (n < h->tstepdenmin) h->tstepdenmin = n;
+  }
+  h->n_fail += (long long)z.n_fail;
+  h->n_iters += (long long)z.n_iters;
+  h->n_solves += (long long)z.n_solves;
+  h->n_guard += (long long)z.n_guard;
+  if (z.err) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "device pass failed with status %d at cell %lld", z.err, z.err_cell);
+    return fail(h, z.err, buf);
+  }
+  return KC_OK;
+}
+
+// Sim.step (koral/sim.zig:1792)
+int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
+  double t = h->t;
+  h->own_dt = 1.0 / h->tstepdenmax;
+  double dt = isnan(forced_dt) ? h->own_dt : forced_dt;
+  h->dt = dt;
+  long long fail0 = h->n_fail;
+  h->tstepdenmax = -1.0;
+  h->tstepdenmin = 1.0e50;
+  reset_step_scalars(h);
+  const double gam_imex = KP_GAM_IMEX;
+  double* u = h->ds.u;
+  if (h->sp.radviscosity) launch_rijvisc(h, dt);
+  // 1st implicit
+  copy_field(h, h->ut0, u);
+  launch_implicit(h, dt * gam_imex);
+  launch_stage_deriv(h, h->drt1, u, h->ut0, dt * gam_imex);
+  // 1st explicit
+  copy_field(h, h->ut1, u);
+  launch_calc_u2p(h);
+  launch_do_correct(h);
+  launch_set_bc(h);
+  launch_op_explicit(h, dt);
+  if (h->sp.dynamo) launch_dynamo(h, dt);
+  {
+    const DGrid& gr = h->gr;
+    k_copy_entropy_count<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds);
+  }
+  launch_stage_deriv(h, h->dut1, u, h->ut1, dt);
+  launch_stage_combine(h, u, h->ut0, dt, h->dut1, dt * KP_ONE_M2GAM, h->drt1);
+  // 2nd implicit
+  copy_field(h, h->uforget, u);
+  launch_calc_u2p(h);
+  launch_do_correct(h);
+  launch_implicit(h, gam_imex * dt);
+  launch_stage_deriv(h, h->drt2, u, h->uforget, dt * gam_imex);
+  // 2nd explicit
+  copy_field(h, h->ut2, u);
+  launch_calc_u2p(h);
+  launch_do_correct(h);
+  launch_set_bc(h);
+  launch_op_explicit(h, dt);
+  if (h->sp.dynamo) launch_dynamo(h, dt);
+  launch_stage_deriv(h, h->dut2, u, h->ut2, dt);
+  launch_stage_combine(h, u, h->ut0, dt / 2.0, h->dut1, dt / 2.0, h->dut2);
+  launch_stage_combine(h, u, u, dt / 2.0, h->drt1, dt / 2.0, h->drt2);
+  launch_calc_u2p(h);
+  launch_do_correct(h);
+  launch_set_bc(h);
+  {
+    const DGrid& gr = h->gr;
+    k_update_entropy<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam);
+  }
+  int st = sync_check(h, "step launch");
+  if (st) return st;
+  st = collect_step_scalars(h, true);
+  h->t = t + dt;
+  h->n_fail_step = h->n_fail - fail0;
+  h->nstep += 1;
+  if (info) {
+    info->dt = dt;
+    info->nan_cell = -1;
+  }
+  return st;
+}
+
+}  // namespace
+
+// ==== C ABI ===================================================================
+extern "C" {
+
+void kc_options_puffy(kc_options* opt) { options_puffy(opt); }
+void kc_grid_puffy(int32_t nx, int32_t ny, int32_t nz, kc_grid* grid) { grid_puffy(nx, ny, nz, grid); }
+
+const char* kc_last_error(const kc_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
+  if (!grid || !opt || !out) return KC_ERR_INVALID_CONFIG;
+  *out = nullptr;
+  const char* why = validate_config(*grid, *opt);
+  kc_handle* h = new kc_handle();
+  if (why) {
+    fail(h, KC_ERR_INVALID_CONFIG, why);
+    *out = h;
+    return KC_ERR_INVALID_CONFIG;
+  }
+  *out = h;
+  h->kg = *grid;
+  h->opt = *opt;
+  params_from_options(*opt, h->sp);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(h, KC_ERR_NO_DEVICE, "no CUDA device");
+  if (opt->device < 0 || opt->device >= ndev) return fail(h, KC_ERR_INVALID_CONFIG, "device ordinal out of range");
+  int st = cuda_check(h, cudaSetDevice(opt->device), "cudaSetDevice");
+  if (st) return st;
+  st = cuda_check(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (st) return st;
+  Grid g = grid_init(grid->nx, grid->ny, grid->nz, grid->ng, grid->minx, grid->maxx, grid->miny, grid->maxy, grid->minz,
+                     grid->maxz);
+  DGrid& gr = h->gr;
+  gr.g = g;
+  gr.nx = g.nx;
+  gr.ny = g.ny;
+  gr.nz = g.nz;
+  gr.ng = g.ng;
+  gr.ngx = g.ngx;
+  gr.ngy = g.ngy;
+  gr.ngz = g.ngz;
+  gr.sx = g.nx + 2 * g.ngx;
+  gr.sy = g.ny + 2 * g.ngy;
+  gr.sz = g.nz + 2 * g.ngz;
+  gr.nc = gr.sx * gr.sy * gr.sz;
+  h->ds.gr = gr;
+  for (int d = 0; d < 3; ++d) h->ds.nf[d] = (gr.sx + (d == 0)) * (gr.sy + (d == 1)) * (gr.sz + (d == 2));
+  st = build_cache(h);
+  if (st) return st;
+  long nc = gr.nc;
+  h->ds.p = dalloc<double>(h, NV * nc, st);
+  h->ds.u = dalloc<double>(h, NV * nc, st);
+  h->ds.flags = dalloc<int>(h, 6 * nc, st);
+  h->ds.amax = dalloc<double>(h, 6 * nc, st);
+  for (int d = 0; d < 3; ++d) h->ds.flb[d] = dalloc<double>(h, NV * h->ds.nf[d], st);
+  for (int d = 0; d < 3; ++d) h->ds.emf[d] = dalloc<double>(h, (size_t)(gr.nx + 1) * (gr.ny + 1) * (gr.nz + 1), st);
+  h->ds.rijvisc = dalloc<double>(h, 16 * nc, st);
+  h->ds.dyn_a = dalloc<double>(h, nc, st);
+  h->ds.vecpot = dalloc<double>(h, 6 * nc, st);
+  h->ds.scaleth = dalloc<double>(h, gr.nx, st);
+  h->ds.fix_p = dalloc<double>(h, NV * nc, st);
+  h->ds.fix_u = dalloc<double>(h, NV * nc, st);
+  h->ut0 = dalloc<double>(h, NV * nc, st);
+  h->ut1 = dalloc<double>(h, NV * nc, st);
+  h->ut2 = dalloc<double>(h, NV * nc, st);
+  h->dut1 = dalloc<double>(h, NV * nc, st);
+  h->dut2 = dalloc<double>(h, NV * nc, st);
+  h->drt1 = dalloc<double>(h, NV * nc, st);
+  h->drt2 = dalloc<double>(h, NV * nc, st);
+  h->uforget = dalloc<double>(h, NV * nc, st);
+  h->staging = dalloc<double>(h, NV * nc, st);
+  h->flag_staging = dalloc<int>(h, 6 * nc, st);
+  h->dsc = dalloc<DevScalars>(h, 1, st);
+  if (st) return st;
+  // set_grid min-size scan with C's mdx quirk (koral/sim.zig:443)
+  double mdx = -1, mdy = -1, mdz = -1;
+  for (long ix = 0; ix < g.nx; ++ix)
+    for (long iy = 0; iy < g.ny; ++iy)
+      for (long iz = 0; iz < g.nz; ++iz) {
+        double dx = cell_size(g, ix, 0), dy = cell_size(g, iy, 1), dz = cell_size(g, iz, 2);
+        if (dx < mdx || mdx < 0) mdx = dx;
+        if (dy < mdx || mdy < 0) mdy = dy;
+        if (dz < mdx || mdz < 0) mdz = dz;
+      }
+  h->min_dx = mdx;
+  h->min_dy = mdy;
+  h->min_dz = mdz;
+  return cuda_check(h, cudaDeviceSynchronize(), "kc_create");
+}
+
+void kc_destroy(kc_handle* h) {
+  if (!h) return;
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+static int upload_field(kc_handle* h, double* dst, const double* host, int nv) {
+  if (!h || !host) return KC_ERR_INVALID_CONFIG;
+  long n = (long)nv * h->gr.nc;
+  int st = cuda_check(h, cudaMemcpyAsync(h->staging, host, n * 8, cudaMemcpyHostToDevice, h->stream), "upload");
+  if (st) return st;
+  k_aos_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->staging, dst, h->gr.nc, nv);
+  return cuda_check(h, cudaStreamSynchronize(h->stream), "upload");
+}
+static int download_field(kc_handle* h, const double* src, double* host, int nv) {
+  if (!h || !host) return KC_ERR_INVALID_CONFIG;
+  long n = (long)nv * h->gr.nc;
+  k_soa_to_aos<<<nblk(n, 256), 256, 0, h->stream>>>(src, h->staging, h->gr.nc, nv);
+  int st = cuda_check(h, cudaMemcpyAsync(host, h->staging, n * 8, cudaMemcpyDeviceToHost, h->stream), "download");
+  if (st) return st;
+  return cuda_check(h, cudaStreamSynchronize(h->stream), "download");
+}
+
+int kc_upload_prims(kc_handle* h, const double* p) { return upload_field(h, h->ds.p, p, NV); }
+int kc_upload_cons(kc_handle* h, const double* u) { return upload_field(h, h->ds.u, u, NV); }
+int kc_download_prims(kc_handle* h, double* p) { return download_field(h, h->ds.p, p, NV); }
+int kc_download_cons(kc_handle* h, double* u) { return download_field(h, h->ds.u, u, NV); }
+int kc_upload_flags(kc_handle* h, const int32_t* f) {
+  if (!h || !f) return KC_ERR_INVALID_CONFIG;
+  long n = 6L * h->gr.nc;
+  int st = cuda_check(h, cudaMemcpyAsync(h->flag_staging, f, n * 4, cudaMemcpyHostToDevice, h->stream), "upload");
+  if (st) return st;
+  k_flags_to_soa<<<nblk(n, 256), 256, 0, h->stream>>>(h->flag_staging, h->ds.flags, h->gr.nc);
+  return cuda_check(h, cudaStreamSynchronize(h->stream), "upload");
+}
+int kc_download_flags(kc_handle* h, int32_t* f) {
+  if (!h || !f) return KC_ERR_INVALID_CONFIG;
+  long n = 6L * h->gr.nc;
+  k_flags_to_aos<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds.flags, h->flag_staging, h->gr.nc);
+  int st = cuda_check(h, cudaMemcpyAsync(f, h->flag_staging, n * 4, cudaMemcpyDeviceToHost, h->stream), "download");
+  if (st) return st;
+  return cuda_check(h, cudaStreamSynchronize(h->stream), "download");
+}
+
+int kc_set_counters(kc_handle* h, const kc_counters* c) {
+  if (!h || !c) return KC_ERR_INVALID_CONFIG;
+  h->t = c->t;
+  h->dt = c->dt;
+  h->own_dt = c->own_dt;
+  h->tstepdenmax = c->tstepdenmax;
+  h->tstepdenmin = c->tstepdenmin;
+  h->nstep = c->nstep;
+  h->n_fail = c->n_radimp_failures;
+  h->n_fail_step = c->n_radimp_fail_step;
+  h->n_iters = c->n_radimp_iters;
+  h->n_solves = c->n_radimp_solves;
+  h->n_guard = c->n_guard_recoveries;
+  return KC_OK;
+}
+int kc_get_counters(kc_handle* h, kc_counters* c) {
+  if (!h || !c) return KC_ERR_INVALID_CONFIG;
+  c->t = h->t;
+  c->dt = h->dt;
+  c->own_dt = h->own_dt;
+  c->tstepdenmax = h->tstepdenmax;
+  c->tstepdenmin = h->tstepdenmin;
+  c->nstep = h->nstep;
+  c->n_radimp_failures = h->n_fail;
+  c->n_radimp_fail_step = h->n_fail_step;
+  c->n_radimp_iters = h->n_iters;
+  c->n_radimp_solves = h->n_solves;
+  c->n_guard_recoveries = h->n_guard;
+  return KC_OK;
+}
+
+int kc_init_timestep_guess(kc_handle* h) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  const double ws = 10000.0;
+  double tsd;
+  if (h->gr.nz > 1) tsd = ws / h->min_dx + ws / h->min_dy + ws / h->min_dz;
+  else if (h->gr.ny > 1) tsd = ws / h->min_dx + ws / h->min_dy;
+  else tsd = ws / h->min_dx;
+  tsd /= h->sp.tsteplim;
+  h->tstepdenmax = tsd;
+  h->tstepdenmin = tsd;
+  return KC_OK;
+}
+
+int kc_set_bc(kc_handle* h) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  reset_step_scalars(h);
+  launch_set_bc(h);
+  int st = sync_check(h, "set_bc");
+  return st ? st : collect_step_scalars(h, false);
+}
+int kc_calc_u2p(kc_handle* h) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  reset_step_scalars(h);
+  launch_calc_u2p(h);
+  int st = sync_check(h, "calc_u2p");
+  return st ? st : collect_step_scalars(h, false);
+}
+int kc_finish_init(kc_handle* h) {
+  int st = kc_set_bc(h);
+  if (st) return st;
+  return kc_init_timestep_guess(h);
+}
+int kc_cfl_dt(kc_handle* h, double* dt) {
+  if (!h || !dt) return KC_ERR_INVALID_CONFIG;
+  *dt = 1.0 / h->tstepdenmax;
+  return KC_OK;
+}
+int kc_step(kc_handle* h, double forced_dt, kc_step_info* info) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (h->last_status) return h->last_status;
+  return run_step(h, forced_dt, info);
+}
+int kc_step_n(kc_handle* h, int32_t nsteps, double forced_dt) {
+  for (int i = 0; i < nsteps; ++i) {
+    int st = kc_step(h, forced_dt, nullptr);
+    if (st) return st;
+  }
+  return KC_OK;
+}
+
+// debugging surface for the parity tests: run one pass
+int kc_debug_phase(kc_handle* h, int phase, double dt) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  reset_step_scalars(h);
+  switch (phase) {
+    case 0: launch_wavespeeds(h); break;
+    case 1: launch_face_fluxes(h); break;
+    case 2: launch_flux_ct(h); break;
+    case 3: {
+      const DGrid& gr = h->gr;
+      k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dt);
+      break;
+    }
+    case 4: launch_calc_u2p(h); break;
+    case 5: launch_implicit(h, dt); break;
+    case 6: launch_rijvisc(h, dt); break;
+    case 7: launch_dynamo(h, dt); break;
+    case 8: launch_do_correct(h); break;
+    case 9: launch_op_explicit(h, dt); break;
+    default: return KC_ERR_INVALID_CONFIG;
+  }
+  int st = sync_check(h, "phase");
+  if (st) return st;
+  return collect_step_scalars(h, phase == 0 || phase == 9);
+}
+int kc_debug_get_array(kc_handle* h, int which, double* out) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  const double* src = nullptr;
+  size_t n = 0;
+  switch (which) {
+    case 1: src = h->ds.rijvisc; n = 16 * h->gr.nc; break;
+    case 2: src = h->ds.flb[0]; n = NV * h->ds.nf[0]; break;
+    case 3: src = h->ds.flb[1]; n = NV * h->ds.nf[1]; break;
+    case 4: src = h->ds.flb[2]; n = NV * h->ds.nf[2]; break;
+    case 5: src = h->ds.scaleth; n = h->gr.nx; break;
+    case 10: src = h->ds.amax; n = 6 * h->gr.nc; break;
+    default: return KC_ERR_INVALID_CONFIG;
+  }
+  cudaMemcpy(out, src, n * 8, cudaMemcpyDeviceToHost);
+  return (int)n;
+}
+
+int kc_set_precision(kc_handle* h, int32_t mode) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (mode != KC_PLAIN_FP64) return fail(h, KC_ERR_INVALID_CONFIG, "precision mode not built");
+  h->opt.precision = mode;
+  return KC_OK;
+}
+int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (mode != KC_IMPLICIT_PER_CELL) return fail(h, KC_ERR_INVALID_CONFIG, "implicit mode not built");
+  h->opt.implicit_mode = mode;
+  return KC_OK;
+}
+int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweights) {
+  (void)weights;
+  (void)nweights;
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (mode != KC_GUESS_PLAIN) return fail(h, KC_ERR_INVALID_CONFIG, "learned guess not built");
+  return KC_OK;
+}
+int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed) {
+  (void)perturb;
+  (void)perturb_rho;
+  (void)seed;
+  return fail(h, KC_ERR_INVALID_CONFIG, "PUFFY init not built");
+}
+
+}  // extern "C"
+
+// ==== batched per-cell entry points ============================================
+namespace {
+
+// golden-record geometry: gg and GG upper triangles, gdet, alpha, gttpert
+// (koral/testing/golden.zig:241 geomFromRecord)
+__device__ void geom_from_record23(const double* v, Geom& g) {
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 5; ++j) {
+      g.gg[i][j] = 0.0;
+      g.GG[i][j] = 0.0;
+    }
+  int n = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) {
+      g.gg[i][j] = v[n];
+      g.gg[j][i] = v[n];
+      g.GG[i][j] = v[10 + n];
+      g.GG[j][i] = v[10 + n];
+      ++n;
+    }
+  g.gdet = v[20];
+  g.alpha = v[21];
+  g.gttpert = v[22];
+  for (int i = 0; i < 4; ++i) g.xx[i] = 0.0;
+}
+
+struct BatchArgs {
+  double gam;
+  RadParams rp;
+  OpacParams op;
+  ImplicitParams ip;
+  FloorParams fl;
+};
+
+__global__ void __launch_bounds__(128) k_implicit_batch(long n, const double* __restrict__ geom23,
+                                                        const double* __restrict__ dt, double* pp_io, int* res,
+                                                        BatchArgs a) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Geom g;
+  geom_from_record23(geom23 + i * 23, g);
+  double pp[NV], uu[NV];
+  for (int k = 0; k < NV; ++k) pp[k] = pp_io[i * NV + k];
+  ImplicitResult r = solve_implicit_lab(uu, pp, g, dt[i], a.gam, a.rp, a.op, a.ip);
+  for (int k = 0; k < NV; ++k) pp_io[i * NV + k] = pp[k];
+  int* o = res + i * 6;
+  o[0] = r.ok;
+  o[1] = r.rung;
+  o[2] = r.iters;
+  o[3] = r.whichprim;
+  o[4] = r.whicheq;
+  o[5] = r.whichframe;
+}
+
+__global__ void __launch_bounds__(128) k_u2p_batch(long n, const double* __restrict__ geom23,
+                                                   const double* __restrict__ uu_in, double* pp_io, int* fl_out,
+                                                   BatchArgs a) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Geom g;
+  geom_from_record23(geom23 + i * 23, g);
+  double pp[NV], uu[NV];
+  for (int k = 0; k < NV; ++k) {
+    pp[k] = pp_io[i * NV + k];
+    uu[k] = uu_in[i * NV + k];
+  }
+  U2pMhdRes res = u2p_mhd(uu, pp, g, a.gam, a.fl);
+  U2pRadRes rr = u2p_rad(uu, pp, g, a.rp);
+  int gc = 0;
+  check_floors_mhd(pp, g, a.gam, a.fl, gc);
+  check_floors_rad(pp, g, a.rp);
+  for (int k = 0; k < NV; ++k) pp_io[i * NV + k] = pp[k];
+  fl_out[i * 3 + 0] = res.entropy_used;
+  fl_out[i * 3 + 1] = res.fixup;
+  fl_out[i * 3 + 2] = rr.corrected ? -1 : 0;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+int batch_prepare(const kc_options* opt, BatchArgs& a) {
+  if (!opt || opt->abi_version != KC_ABI_VERSION) return KC_ERR_INVALID_CONFIG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return KC_ERR_NO_DEVICE;
+  if (cudaSetDevice(opt->device) != cudaSuccess) return KC_ERR_CUDA;
+  SimParams sp;
+  params_from_options(*opt, sp);
+  a.gam = sp.gam;
+  a.rp = sp.rp;
+  a.op = sp.op;
+  a.ip = sp.ip;
+  a.fl = sp.fl;
+  return KC_OK;
+}
+
+}  // namespace
+
+extern "C" int kc_implicit_batch(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
+                                 int32_t* res, int32_t mode) {
+  BatchArgs a;
+  int st = batch_prepare(opt, a);
+  if (st) return st;
+  if (mode != KC_IMPLICIT_PER_CELL) return KC_ERR_INVALID_CONFIG;
+  if (n <= 0) return KC_OK;
+  DevBuf dg, dd, dp, dr;
+  if (cudaMalloc(&dg.p, n * 23 * 8) || cudaMalloc(&dd.p, n * 8) || cudaMalloc(&dp.p, n * NV * 8) ||
+      cudaMalloc(&dr.p, n * 6 * 4))
+    return KC_ERR_OOM;
+  cudaMemcpy(dg.p, geom23, n * 23 * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(dd.p, dt, n * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(dp.p, pp, n * NV * 8, cudaMemcpyHostToDevice);
+  k_implicit_batch<<<nblk(n), TPB>>>(n, (const double*)dg.p, (const double*)dd.p, (double*)dp.p, (int*)dr.p, a);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  cudaMemcpy(pp, dp.p, n * NV * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(res, dr.p, n * 6 * 4, cudaMemcpyDeviceToHost);
+  return KC_OK;
+}
+
+extern "C" int kc_u2p_batch(const kc_options* opt, int64_t n, const double* geom23, const double* uu, double* pp,
+                            int32_t* flags_out) {
+  BatchArgs a;
+  int st = batch_prepare(opt, a);
+  if (st) return st;
+  if (n <= 0) return KC_OK;
+  DevBuf dg, du, dp, df;
+  if (cudaMalloc(&dg.p, n * 23 * 8) || cudaMalloc(&du.p, n * NV * 8) || cudaMalloc(&dp.p, n * NV * 8) ||
+      cudaMalloc(&df.p, n * 3 * 4))
+    return KC_ERR_OOM;
+  cudaMemcpy(dg.p, geom23, n * 23 * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(du.p, uu, n * NV * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(dp.p, pp, n * NV * 8, cudaMemcpyHostToDevice);
+  k_u2p_batch<<<nblk(n), TPB>>>(n, (const double*)dg.p, (const double*)du.p, (double*)dp.p, (int*)df.p, a);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  cudaMemcpy(pp, dp.p, n * NV * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(flags_out, df.p, n * 3 * 4, cudaMemcpyDeviceToHost);
+  return KC_OK;
+}

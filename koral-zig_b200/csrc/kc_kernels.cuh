@@ -1,0 +1,1099 @@
+// kc_kernels.cuh — the sm_100a kernels of one RK2IMEX step. Each kernel is
+// one pass of the reference's Sim.step (koral/sim.zig:1792) over a grid of
+// cells, faces or corners, calling the shared per-point restatement; the
+// arithmetic of every point is the reference's, so the plain FP64 build
+// (--fmad=false) reproduces the CPU oracle bit for bit.
+#pragma once
+#include "kc_dev.cuh"
+
+namespace kc {
+
+__device__ __forceinline__ void set_err(DevScalars* sc, int code, long long cell) {
+  if (atomicCAS(&sc->err, 0, code) == 0) sc->err_cell = cell;
+}
+__device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// ---- generic cell ranges -----------------------------------------------------
+// A launch covers ix in [x0, x0+nx), iy in [y0, y0+ny), iz in [z0, z0+nz); the
+// thread's x coordinate walks ix so neighbouring lanes touch neighbouring cells.
+struct Range {
+  long x0, y0, z0, nx, ny, nz;
+};
+__device__ __forceinline__ bool range_cell(const Range& r, long& ix, long& iy, long& iz) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long n = r.nx * r.ny * r.nz;
+  if (t >= n) return false;
+  ix = r.x0 + t % r.nx;
+  long q = t / r.nx;
+  iy = r.y0 + q % r.ny;
+  iz = r.z0 + q / r.ny;
+  return true;
+}
+
+// ---- AoS <-> SoA transposes at the host boundary ---------------------------------
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long nc, int nv) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc * nv) return;
+  long c = t / nv;
+  int v = (int)(t % nv);
+  soa[(long)v * nc + c] = aos[t];
+}
+__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, long nc, int nv) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc * nv) return;
+  long c = t / nv;
+  int v = (int)(t % nv);
+  aos[t] = soa[(long)v * nc + c];
+}
+__global__ void k_flags_to_soa(const int* __restrict__ aos, int* __restrict__ soa, long nc) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc * 6) return;
+  soa[(t % 6) * nc + t / 6] = aos[t];
+}
+__global__ void k_flags_to_aos(const int* __restrict__ soa, int* __restrict__ aos, long nc) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc * 6) return;
+  aos[t] = soa[(t % 6) * nc + t / 6];
+}
+
+// ---- stage arithmetic (koral/sim.zig:1586-1709) ------------------------------
+// dst = (1/delta) a + (-1/delta) b over the domain
+__global__ void k_stage_deriv(DevState s, double* dst, const double* a, const double* b, double delta) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long c = cidx(s.gr, ix, iy, iz);
+  double f1 = 1.0 / delta, f2 = -1.0 / delta;
+  long nc = s.gr.nc;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) dst[iv * nc + c] = f1 * a[iv * nc + c] + f2 * b[iv * nc + c];
+}
+// dst = a + f1 b + f2 cc over the domain
+__global__ void k_stage_combine(DevState s, double* dst, const double* a, double f1, const double* b, double f2,
+                                const double* cc) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long c = cidx(s.gr, ix, iy, iz);
+  long nc = s.gr.nc;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) dst[iv * nc + c] = a[iv * nc + c] + f1 * b[iv * nc + c] + f2 * cc[iv * nc + c];
+}
+// flags entropy3 = entropy (C copy_entropycount)
+__global__ void k_copy_entropy_count(DevState s) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long c = cidx(s.gr, ix, iy, iz);
+  s.flags[2 * s.gr.nc + c] = s.flags[0 * s.gr.nc + c];
+}
+// C update_entropy (koral/sim.zig:1683)
+__global__ void __launch_bounds__(128) k_update_entropy(DevState s, double gam) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long c = cidx(s.gr, ix, iy, iz), nc = s.gr.nc;
+  double pp[NV], uu[NV];
+  load_cell(s.p, nc, c, pp);
+  load_cell(s.u, nc, c, uu);
+  pp[ENTR] = s_from_u(pp[RHO], pp[UU], gam);
+  s.p[ENTR * nc + c] = pp[ENTR];
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  p2u_mhd(pp, uu, g, gam);
+#pragma unroll
+  for (int iv = 0; iv < 9; ++iv) s.u[iv * nc + c] = uu[iv];
+}
+
+// ---- u2p (koral/sim.zig:924-1000) --------------------------------------------
+__global__ void __launch_bounds__(128) k_u2p(DevState s, DevScalars* sc, double gam, FloorParams fl, RadParams rp,
+                                             int polar_nc) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long c = cidx(s.gr, ix, iy, iz), nc = s.gr.nc;
+  double uu[NV], pp[NV];
+  load_cell(s.u, nc, c, uu);
+  load_cell(s.p, nc, c, pp);
+  s.flags[0 * nc + c] = 0;
+  s.flags[1 * nc + c] = 0;
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  bool polar = polar_nc > 0 && (iy < polar_nc || iy > s.gr.ny - polar_nc - 1);
+  if (polar) {
+    double gdetu_inv = 1.0 / g.gdet;
+    s.p[B1 * nc + c] = uu[B1] * gdetu_inv;
+    s.p[B2 * nc + c] = uu[B2] * gdetu_inv;
+    s.p[B3 * nc + c] = uu[B3] * gdetu_inv;
+    s.flags[3 * nc + c] = 0;
+    s.flags[4 * nc + c] = 0;
+    return;
+  }
+  U2pMhdRes res = u2p_mhd(uu, pp, g, gam, fl);
+  if (res.entropy_used) s.flags[0 * nc + c] = 1;
+  U2pRadRes rr = u2p_rad(uu, pp, g, rp);
+  int gc = 0;
+  check_floors_mhd(pp, g, gam, fl, gc);
+  if (gc) atomicAdd(&sc->n_guard, (unsigned long long)gc);
+  check_floors_rad(pp, g, rp);
+  store_cell(s.p, nc, c, pp);
+  s.flags[3 * nc + c] = res.fixup ? 1 : 0;
+  s.flags[4 * nc + c] = rr.corrected ? -1 : 0;
+  if (res.fixup) atomicOr(&sc->any_hd, 1);
+}
+
+// cell_fixup(FIXUP_U2PMHD), pass 1: flagged cells average their non-flagged
+// in-domain neighbours into the staging buffers (koral/sim.zig:1067)
+__global__ void __launch_bounds__(128) k_fixup_hd(DevState s, DevScalars* sc, double gam, int polar_nc) {
+  if (!sc->any_hd) return;
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  if (polar_nc > 0 && (iy < polar_nc || iy > s.gr.ny - polar_nc - 1)) return;
+  const int* fhd = s.flags + 3 * nc;
+  if (fhd[c] == 0) return;
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+  long nb[6][3] = {{ix - 1, iy, iz}, {ix + 1, iy, iz}, {ix, iy - 1, iz}, {ix, iy + 1, iz}, {ix, iy, iz - 1}, {ix, iy, iz + 1}};
+  long ncells[6];
+  int in_n = 0;
+  for (int k = 0; k < 6; ++k) {
+    if (nb[k][0] < 0 || nb[k][0] >= nx || nb[k][1] < 0 || nb[k][1] >= ny || nb[k][2] < 0 || nb[k][2] >= nz) continue;
+    long cn = cidx(s.gr, nb[k][0], nb[k][1], nb[k][2]);
+    if (fhd[cn] != 0) continue;
+    ncells[in_n++] = cn;
+  }
+  bool enough = (nz == 1 && ny == 1 && in_n >= 1) || (nz == 1 && in_n >= 2) || (ny == 1 && in_n >= 2) || in_n >= 3;
+  if (!enough) return;
+  double pp[NV];
+  load_cell(s.p, nc, c, pp);
+  for (int iv = 0; iv < NV; ++iv) {
+    if (iv != RHO && iv < B1) {
+      double sum = 0.0;
+      for (int k = 0; k < in_n; ++k) sum += s.p[iv * nc + ncells[k]];
+      pp[iv] = sum / (double)in_n;
+    }
+  }
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  double uu[NV];
+  p2u(pp, uu, g, gam);
+  store_cell(s.fix_p, nc, c, pp);
+  store_cell(s.fix_u, nc, c, uu);
+  // mark the cell as staged; the bit keeps the flag nonzero for the
+  // neighbour tests of concurrent threads and is cleared in pass 2
+  s.flags[3 * nc + c] = fhd[c] | 0x40000000;
+}
+// pass 2: copy the staged cells back
+__global__ void k_fixup_apply(DevState s, DevScalars* sc) {
+  if (!sc->any_hd) return;
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  int f = s.flags[3 * nc + c];
+  if (!(f & 0x40000000)) return;
+  s.flags[3 * nc + c] = f & ~0x40000000;
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) {
+    s.p[iv * nc + c] = s.fix_p[iv * nc + c];
+    s.u[iv * nc + c] = s.fix_u[iv * nc + c];
+  }
+}
+
+// ---- boundary conditions (koral/sim/bc.zig, puffy.zig:1080) ------------------
+__device__ int puffy_bc_cell(const DevState& s, long ix, long iy, long iz, int face, double pp[NV]) {
+  const long nx = s.gr.nx, ny = s.gr.ny, nc = s.gr.nc;
+  if (face == 1) {
+    load_cell(s.p, nc, cidx(s.gr, nx - 1, iy, iz), pp);
+    Geom geo, gbl, gbd;
+    geom_cell(s, ix, iy, iz, geo);
+    long c = cidx(s.gr, ix, iy, iz);
+    geom_bl(s, c, gbl);
+    double jm2b[4][4], jb2m[4][4];
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) jm2b[a][b] = s.jbl[(long)(a * 4 + b) * nc + c];
+    long gi = (ix - nx) + (long)s.gr.ngx * ((iy + s.gr.ngy) + s.gr.sy * (iz + s.gr.ngz));
+    long ngh = (long)s.gr.ngx * s.gr.sy * s.gr.sz;
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) jb2m[a][b] = s.jb2m[(long)(a * 4 + b) * ngh + gi];
+    int e = trans_pmhd_coco_j(pp, geo, gbl, jm2b, pp);
+    if (e) return e;
+    double rghost = gbl.xx[1];
+    double rbound = s.blg[26L * nc + cidx(s.gr, nx - 1, iy, iz)];
+    double scale1 = rbound * rbound / rghost / rghost;
+    double scale2 = rbound / rghost;
+    pp[RHO] *= scale1;
+    pp[UU] *= scale1;
+    pp[B1] *= scale1;
+    pp[B2] *= scale2;
+    pp[B3] *= scale2;
+    pp[VY] *= scale1;
+    pp[VZ] *= scale1;
+    pp[EE] *= scale1;
+    pp[FY] *= scale1;
+    pp[FZ] *= scale1;
+    e = trans_pmhd_coco_j(pp, gbl, geo, jb2m, pp);
+    if (e) return e;
+    double ucon[4] = {0.0, pp[VX], pp[VY], pp[VZ]};
+    velr_to_vel4(ucon, geo, ucon);
+    transform_vec(ucon, jm2b, ucon);
+    if (ucon[1] < 0.0) {
+      ucon[1] = 0.0;
+      transform_vec(ucon, jb2m, ucon);
+      e = convert(ucon, VEL4, VELR, geo, RECOMPUTE_UT, ucon);
+      if (e) return e;
+      pp[VX] = ucon[1];
+      pp[VY] = ucon[2];
+      pp[VZ] = ucon[3];
+    }
+    double urf[4] = {0.0, pp[FX], pp[FY], pp[FZ]};
+    velr_to_vel4(urf, geo, urf);
+    transform_vec(urf, jm2b, urf);
+    if (urf[1] < 0.0) {
+      urf[1] = 0.0;
+      transform_vec(urf, jb2m, urf);
+      e = convert(urf, VEL4, VELR, geo, RECOMPUTE_UT, urf);
+      if (e) return e;
+      pp[FX] = urf[1];
+      pp[FY] = urf[2];
+      pp[FZ] = urf[3];
+    }
+    return E_OK;
+  }
+  if (face == 0) {
+    load_cell(s.p, nc, cidx(s.gr, 0, iy, iz), pp);
+    return E_OK;
+  }
+  long iiy = (face == 2) ? -iy - 1 : ny - (iy - ny) - 1;
+  load_cell(s.p, nc, cidx(s.gr, ix, iiy, iz), pp);
+  pp[VY] = -pp[VY];
+  pp[B2] = -pp[B2];
+  pp[FY] = -pp[FY];
+  return E_OK;
+}
+
+__device__ void bc_cell(const DevState& s, DevScalars* sc, long ix, long iy, long iz, int face, const int bc[3],
+                        double gam) {
+  int axis = face / 2;
+  int kind = bc[axis];
+  long nc = s.gr.nc;
+  double pp[NV];
+  if (kind == KC_BC_PUFFY) {
+    int e = puffy_bc_cell(s, ix, iy, iz, face, pp);
+    if (e) {
+      set_err(sc, e, cidx(s.gr, ix, iy, iz));
+      return;
+    }
+  } else {
+    long iix = ix, iiy = iy, iiz = iz, nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+    if (axis == 0) {
+      if (kind == KC_BC_PERIODIC) {
+        if (ix < 0) iix = ix + nx;
+        if (ix > nx - 1) iix = ix - nx;
+      } else {
+        if (ix < 0) iix = 0;
+        if (ix > nx - 1) iix = nx - 1;
+      }
+    } else if (axis == 1) {
+      if (kind == KC_BC_PERIODIC) {
+        if (iy < 0) iiy = iy + ny;
+        if (iy > ny - 1) iiy = iy - ny;
+        if (ny < s.gr.ng) iiy = 0;
+      } else {
+        if (iy < 0) iiy = 0;
+        if (iy > ny - 1) iiy = ny - 1;
+      }
+    } else {
+      if (kind == KC_BC_PERIODIC) {
+        if (iz < 0) iiz = iz + nz;
+        if (iz > nz - 1) iiz = iz - nz;
+        if (nz < s.gr.ng) iiz = 0;
+      } else {
+        if (iz < 0) iiz = 0;
+        if (iz > nz - 1) iiz = nz - 1;
+      }
+    }
+    load_cell(s.p, nc, cidx(s.gr, iix, iiy, iiz), pp);
+  }
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  double uu[NV];
+  p2u(pp, uu, g, gam);
+  long c = cidx(s.gr, ix, iy, iz);
+  store_cell(s.p, nc, c, pp);
+  store_cell(s.u, nc, c, uu);
+}
+
+struct BcArgs {
+  int bc[3];
+  double gam;
+};
+// ghost faces of one axis; thread t -> (ghost layer i, two transverse indices)
+__global__ void __launch_bounds__(128) k_bc_faces(DevState s, DevScalars* sc, BcArgs a, int axis) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+  if (axis == 0) {
+    long ng = s.gr.ngx;
+    long n = 2 * ng * ny * nz;
+    if (t >= n) return;
+    long side = t % 2, q = t / 2;
+    long i = 1 + q % ng;
+    q /= ng;
+    long iy = q % ny, iz = q / ny;
+    if (side == 0) bc_cell(s, sc, -i, iy, iz, 0, a.bc, a.gam);
+    else bc_cell(s, sc, nx - 1 + i, iy, iz, 1, a.bc, a.gam);
+  } else if (axis == 1) {
+    long ng = s.gr.ngy;
+    long n = 2 * ng * nx * nz;
+    if (t >= n) return;
+    long ix = t % nx, q = t / nx;
+    long side = q % 2;
+    q /= 2;
+    long i = 1 + q % ng, iz = q / ng;
+    if (side == 0) bc_cell(s, sc, ix, -i, iz, 2, a.bc, a.gam);
+    else bc_cell(s, sc, ix, ny - 1 + i, iz, 3, a.bc, a.gam);
+  } else {
+    long ng = s.gr.ngz;
+    long n = 2 * ng * nx * ny;
+    if (t >= n) return;
+    long ix = t % nx, q = t / nx;
+    long iy = q % ny;
+    q /= ny;
+    long side = q % 2, i = 1 + q / 2;
+    if (side == 0) bc_cell(s, sc, ix, iy, -i, 4, a.bc, a.gam);
+    else bc_cell(s, sc, ix, iy, nz - 1 + i, 5, a.bc, a.gam);
+  }
+}
+
+__device__ void p2u_cell(const DevState& s, long ix, long iy, long iz, double gam) {
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  double pp[NV], uu[NV];
+  load_cell(s.p, nc, c, pp);
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  p2u(pp, uu, g, gam);
+  store_cell(s.u, nc, c, uu);
+}
+__device__ void copy_p_cell(const DevState& s, long dx, long dy, long dz, long sx_, long sy_, long sz_) {
+  long nc = s.gr.nc, d = cidx(s.gr, dx, dy, dz), c = cidx(s.gr, sx_, sy_, sz_);
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) s.p[iv * nc + d] = s.p[iv * nc + c];
+}
+__device__ void avg_p_cell(const DevState& s, const long d[3], const long a[3], const long b[3]) {
+  long nc = s.gr.nc, cd = cidx(s.gr, d[0], d[1], d[2]), ca = cidx(s.gr, a[0], a[1], a[2]),
+       cb = cidx(s.gr, b[0], b[1], b[2]);
+  double v[NV];
+  for (int iv = 0; iv < NV; ++iv) v[iv] = 0.5 * (s.p[iv * nc + ca] + s.p[iv * nc + cb]);
+  store_cell(s.p, nc, cd, v);
+}
+
+// 2D corner surfaces + diagonals (bc.zig:256): one thread per corner, the
+// strip -> diagonal order inside a corner kept serial
+__global__ void k_corners_2d(DevState s, BcArgs a) {
+  int corner = threadIdx.x;
+  if (corner >= 4) return;
+  long nx = s.gr.nx, ny = s.gr.ny, ng = s.gr.ng;
+  bool px = a.bc[0] == KC_BC_PERIODIC, py = a.bc[1] == KC_BC_PERIODIC;
+  bool xh = corner & 1, yh = corner & 2;
+  for (long i = 0; i < ng - 1; ++i) {
+    long ax = xh ? nx + i + 1 : -ng + i, ay = yh ? ny : -1, asy = yh ? ny - 1 : 0;
+    copy_p_cell(s, ax, ay, 0, ax, asy, 0);
+    p2u_cell(s, ax, ay, 0, a.gam);
+    long bx = xh ? nx : -1, bsx = xh ? nx - 1 : 0, by = yh ? ny + i + 1 : -ng + i;
+    copy_p_cell(s, bx, by, 0, bsx, by, 0);
+    p2u_cell(s, bx, by, 0, a.gam);
+  }
+  long s1[4], s2[4], d1[3], d2[3];
+  if (!xh && !yh) {
+    long t1[4] = {-1, 0, 0, -1}, t2[4] = {-2, -1, -1, -2};
+    if (py) { t1[0] = -1; t1[1] = ny - 1; t1[2] = -1; t1[3] = ny - 1; t2[0] = -2; t2[1] = ny - 2; t2[2] = -2; t2[3] = ny - 2; }
+    if (px) { t1[0] = nx - 1; t1[1] = -1; t1[2] = nx - 1; t1[3] = -1; t2[0] = nx - 2; t2[1] = -2; t2[2] = nx - 2; t2[3] = -2; }
+    for (int k = 0; k < 4; ++k) { s1[k] = t1[k]; s2[k] = t2[k]; }
+    d1[0] = -1; d1[1] = -1; d2[0] = -2; d2[1] = -2;
+  } else if (!xh && yh) {
+    long t1[4] = {-1, ny - 1, 0, ny}, t2[4] = {-2, ny, -1, ny + 1};
+    if (py) { t1[0] = -1; t1[1] = 0; t1[2] = -1; t1[3] = 0; t2[0] = -2; t2[1] = 1; t2[2] = -2; t2[3] = 1; }
+    if (px) { t1[0] = nx - 1; t1[1] = ny; t1[2] = nx - 1; t1[3] = ny; t2[0] = nx - 2; t2[1] = ny + 1; t2[2] = nx - 2; t2[3] = ny + 1; }
+    for (int k = 0; k < 4; ++k) { s1[k] = t1[k]; s2[k] = t2[k]; }
+    d1[0] = -1; d1[1] = ny; d2[0] = -2; d2[1] = ny + 1;
+  } else if (xh && !yh) {
+    long t1[4] = {nx - 1, -1, nx, 0}, t2[4] = {nx, -2, nx + 1, -1};
+    if (py) { t1[0] = nx; t1[1] = ny - 1; t1[2] = nx; t1[3] = ny - 1; t2[0] = nx + 1; t2[1] = ny - 2; t2[2] = nx + 1; t2[3] = ny - 2; }
+    if (px) { t1[0] = 0; t1[1] = -1; t1[2] = 0; t1[3] = -1; t2[0] = 1; t2[1] = -2; t2[2] = 1; t2[3] = -2; }
+    for (int k = 0; k < 4; ++k) { s1[k] = t1[k]; s2[k] = t2[k]; }
+    d1[0] = nx; d1[1] = -1; d2[0] = nx + 1; d2[1] = -2;
+  } else {
+    long t1[4] = {nx - 1, ny, nx, ny - 1}, t2[4] = {nx, ny + 1, nx + 1, ny};
+    if (py) { t1[0] = nx; t1[1] = 0; t1[2] = nx; t1[3] = 0; t2[0] = nx + 1; t2[1] = 1; t2[2] = nx + 1; t2[3] = 1; }
+    if (px) { t1[0] = 0; t1[1] = ny; t1[2] = 0; t1[3] = ny; t2[0] = 1; t2[1] = ny + 1; t2[2] = 1; t2[3] = ny + 1; }
+    for (int k = 0; k < 4; ++k) { s1[k] = t1[k]; s2[k] = t2[k]; }
+    d1[0] = nx; d1[1] = ny; d2[0] = nx + 1; d2[1] = ny + 1;
+  }
+  d1[2] = 0;
+  d2[2] = 0;
+  long a1[3] = {s1[0], s1[1], 0}, b1[3] = {s1[2], s1[3], 0};
+  avg_p_cell(s, d1, a1, b1);
+  p2u_cell(s, d1[0], d1[1], 0, a.gam);
+  long a2[3] = {s2[0], s2[1], 0}, b2[3] = {s2[2], s2[3], 0};
+  avg_p_cell(s, d2, a2, b2);
+  p2u_cell(s, d2[0], d2[1], 0, a.gam);
+}
+
+// one group of four 3D edge tubes (bc.zig:404): thread -> (tube, slice)
+__global__ void k_edge_tubes(DevState s, double gam, int pa, int pb, int pc) {
+  long dims[3] = {s.gr.nx, s.gr.ny, s.gr.nz};
+  long ng = s.gr.ng;
+  long nslice = dims[pc] + 2 * ng;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 4 * nslice) return;
+  int tube = (int)(t / nslice);
+  long cc = -ng + t % nslice;
+  bool a_hi = tube & 2, b_hi = tube & 1;
+  long na = dims[pa], nb = dims[pb];
+  long a_edge = a_hi ? na - 1 : 0, a_g1 = a_hi ? na : -1, a_g2 = a_hi ? na + 1 : -2;
+  long b_edge = b_hi ? nb - 1 : 0, b_g1 = b_hi ? nb : -1, b_g2 = b_hi ? nb + 1 : -2;
+  auto cell = [&](long av, long bv, long cv, long o[3]) {
+    o[pa] = av;
+    o[pb] = bv;
+    o[pc] = cv;
+  };
+  for (long i = 0; i < ng - 1; ++i) {
+    long a_out = a_hi ? na + i + 1 : -ng + i;
+    long b_out = b_hi ? nb + i + 1 : -ng + i;
+    long d[3], src[3];
+    cell(a_out, b_g1, cc, d);
+    cell(a_out, b_edge, cc, src);
+    copy_p_cell(s, d[0], d[1], d[2], src[0], src[1], src[2]);
+    p2u_cell(s, d[0], d[1], d[2], gam);
+    cell(a_g1, b_out, cc, d);
+    cell(a_edge, b_out, cc, src);
+    copy_p_cell(s, d[0], d[1], d[2], src[0], src[1], src[2]);
+    p2u_cell(s, d[0], d[1], d[2], gam);
+  }
+  long d1[3], x1[3], y1[3];
+  cell(a_g1, b_g1, cc, d1);
+  cell(a_g1, b_edge, cc, x1);
+  cell(a_edge, b_g1, cc, y1);
+  avg_p_cell(s, d1, x1, y1);
+  p2u_cell(s, d1[0], d1[1], d1[2], gam);
+  long d2[3], x2[3], y2[3];
+  cell(a_g2, b_g2, cc, d2);
+  cell(a_g2, b_g1, cc, x2);
+  cell(a_g1, b_g2, cc, y2);
+  avg_p_cell(s, d2, x2, y2);
+  p2u_cell(s, d2[0], d2[1], d2[2], gam);
+}
+// the 8 corner cubes (bc.zig:457), in the reference's cube order
+__global__ void k_corner_cubes(DevState s, double gam) {
+  long ng = s.gr.ng;
+  long per = ng * ng * ng;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per) return;
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+  for (int cube = 0; cube < 8; ++cube) {
+    bool xh = cube & 1, yh = cube & 2, zh = cube & 4;
+    long ix = (xh ? nx : -ng) + t % ng, iy = (yh ? ny : -ng) + (t / ng) % ng, iz = (zh ? nz : -ng) + t / (ng * ng);
+    copy_p_cell(s, ix, iy, iz, xh ? nx - 1 : 0, yh ? ny - 1 : 0, zh ? nz - 1 : 0);
+    p2u_cell(s, ix, iy, iz, gam);
+  }
+}
+
+// ---- polar axis overwrite (koral/sim/polaraxis.zig:124) -----------------------
+__global__ void __launch_bounds__(128) k_polar_correct(DevState s, double gam, int ncp) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz, nc = s.gr.nc;
+  if (t >= nx * nz * 2 * ncp) return;
+  long ix = t % nx, q = t / nx;
+  long k = q % (2 * ncp), iz = q / (2 * ncp);
+  long ic = k / 2;
+  long iy = (k % 2 == 0) ? ic : ny - 1 - ic;
+  long iysrc = (iy < ncp) ? ncp : ny - 1 - ncp;
+  double thaxis = grid_yl(s.gr.g, (iy < ncp) ? 0 : ny);
+  double fac = kmath::fabs((grid_yc(s.gr.g, iy) - thaxis) / (grid_yc(s.gr.g, iysrc) - thaxis));
+  long c = cidx(s.gr, ix, iy, iz), cs = cidx(s.gr, ix, iysrc, iz);
+  double pp[NV], pps[NV];
+  load_cell(s.p, nc, c, pp);
+  load_cell(s.p, nc, cs, pps);
+  pp[RHO] = pps[RHO];
+  pp[UU] = pps[UU];
+  pp[ENTR] = pps[ENTR];
+  pp[VX] = pps[VX];
+  pp[VZ] = pps[VZ];
+  pp[VY] = fac * pps[VY];
+  pp[EE] = pps[EE];
+  pp[FX] = pps[FX];
+  pp[FZ] = pps[FZ];
+  pp[FY] = fac * pps[FY];
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  double uu[NV];
+  p2u(pp, uu, g, gam);
+  store_cell(s.p, nc, c, pp);
+  store_cell(s.u, nc, c, uu);
+}
+
+// ---- wavespeeds + CFL reduction (koral/sim.zig:747-886) ----------------------
+struct WsArgs {
+  double gam, tsteplim;
+  OpacParams op;
+  int damp_nc;
+};
+__global__ void __launch_bounds__(128) k_wavespeeds(DevState s, DevScalars* sc, WsArgs a) {
+  const Grid& g = s.gr.g;
+  bool act[3] = {s.gr.nx > 1, s.gr.ny > 1, s.gr.nz > 1};
+  long lx = act[0], ly = act[1], lz = act[2];
+  Range r = {-lx, -ly, -lz, s.gr.nx + 2 * lx, s.gr.ny + 2 * ly, s.gr.nz + 2 * lz};
+  long ix, iy, iz;
+  double tsd = -1.0;
+  if (range_cell(r, ix, iy, iz)) {
+    long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+    double pp[NV];
+    load_cell(s.p, nc, c, pp);
+    Geom geo;
+    geom_cell(s, ix, iy, iz, geo);
+    double aaa[6];
+    gas_wavespeeds_lr(pp, geo, a.gam, act, aaa);
+    double tautot[3];
+    double chi = calc_chi_slim(pp, geo, a.gam, a.op);
+    long idx3[3] = {ix, iy, iz};
+    for (int d = 0; d < 3; ++d) {
+      double sg = kmath::sqrt(geo.gg[d + 1][d + 1]);
+      double dxp = kmath::fmax(cell_size(g, idx3[d], d) * sg, cell_size(g, idx3[d] + 1, d) * sg);
+      tautot[d] = chi * dxp;
+    }
+    if (a.damp_nc > 0 && (iy < a.damp_nc || iy >= s.gr.ny - a.damp_nc)) tautot[0] = tautot[1] = tautot[2] = 0.0;
+    double aval[12], rad0[6], radl[6];
+    rad_wavespeeds(pp, geo, tautot, act, aval);
+    for (int i = 0; i < 6; ++i) {
+      rad0[i] = aval[i];
+      radl[i] = aval[6 + i];
+    }
+    for (int d = 0; d < 3; ++d) {
+      if (radl[2 * d] > 0.0) radl[2 * d] = 0.0;
+      if (radl[2 * d + 1] < 0.0) radl[2 * d + 1] = 0.0;
+      if (rad0[2 * d] > 0.0) rad0[2 * d] = 0.0;
+      if (rad0[2 * d + 1] < 0.0) rad0[2 * d + 1] = 0.0;
+    }
+    double ax = kmath::fmax(kmath::fabs(aaa[0]), kmath::fabs(aaa[1]));
+    double ay = kmath::fmax(kmath::fabs(aaa[2]), kmath::fabs(aaa[3]));
+    double az = kmath::fmax(kmath::fabs(aaa[4]), kmath::fabs(aaa[5]));
+    s.amax[0 * nc + c] = ax;
+    s.amax[1 * nc + c] = ay;
+    s.amax[2 * nc + c] = az;
+    for (int d = 0; d < 3; ++d)
+      s.amax[(3 + d) * nc + c] = kmath::fmax(kmath::fabs(radl[2 * d]), kmath::fabs(radl[2 * d + 1]));
+    double wsx = kmath::fmax(ax, kmath::fmax(kmath::fabs(rad0[0]), kmath::fabs(rad0[1])));
+    double wsy = kmath::fmax(ay, kmath::fmax(kmath::fabs(rad0[2]), kmath::fabs(rad0[3])));
+    double wsz = kmath::fmax(az, kmath::fmax(kmath::fabs(rad0[4]), kmath::fabs(rad0[5])));
+    bool in_domain = ix >= 0 && ix < s.gr.nx && iy >= 0 && iy < s.gr.ny && iz >= 0 && iz < s.gr.nz;
+    if (in_domain) {
+      double dx = cell_size(g, ix, 0), dy = cell_size(g, iy, 1), dz = cell_size(g, iz, 2);
+      if (s.gr.nz > 1 && s.gr.ny > 1) tsd = wsx / dx + wsy / dy + wsz / dz;
+      else if (s.gr.nz == 1 && s.gr.ny > 1) tsd = wsx / dx + wsy / dy;
+      else if (s.gr.ny == 1 && s.gr.nz > 1) tsd = wsx / dx + wsz / dz;
+      else tsd = wsx / dx;
+      tsd /= a.tsteplim;
+      if (!(tsd == tsd)) tsd = -1.0;  // a NaN never wins the reference's max/min
+    }
+  }
+  // block max/min of the positive CFL denominators, then one atomic per block
+  double vmax = tsd > 0.0 ? tsd : 0.0;
+  double vmin = tsd > 0.0 ? tsd : 1.0e300;
+  for (int o = 16; o > 0; o >>= 1) {
+    vmax = fmax(vmax, __shfl_down_sync(0xffffffff, vmax, o));
+    vmin = fmin(vmin, __shfl_down_sync(0xffffffff, vmin, o));
+  }
+  __shared__ double smax[32], smin[32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smax[warp] = vmax;
+    smin[warp] = vmin;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0, n = 1.0e300;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      m = fmax(m, smax[w]);
+      n = fmin(n, smin[w]);
+    }
+    if (m > 0.0) atomicMax(&sc->tsd_max_bits, dbits(m));
+    if (n < 1.0e300) atomicMin(&sc->tsd_min_bits, dbits(n));
+  }
+}
+
+// ---- face fluxes: reconstruct + floors + flux + LAXF (sim.zig:1209-1503) -----
+struct FluxArgs {
+  double gam, theta, maxvel;
+  FloorParams fl;
+  int radvisc;
+};
+__device__ __forceinline__ void face_rijvisc(const DevState& s, long c, long cm, double rv[4][4]) {
+  long nc = s.gr.nc;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) rv[i][j] = 0.5 * (s.rijvisc[(long)(i * 4 + j) * nc + c] + s.rijvisc[(long)(i * 4 + j) * nc + cm]);
+}
+// one face state: floors, one-sided flux, viscous addition, conserveds
+__device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, int dim, double pp[NV], const Geom& g,
+                          long c, long cm, double ff[NV], double uu[NV]) {
+  int gc = 0;
+  check_floors_mhd(pp, g, a.gam, a.fl, gc);
+  if (gc) atomicAdd(&sc->n_guard, (unsigned long long)gc);
+  int e = f_flux_prime(pp, dim, g, a.gam, ff);
+  if (e) return e;
+  p2u(pp, uu, g, a.gam);
+  if (a.radvisc) {
+    double rv[4][4];
+    face_rijvisc(s, c, cm, rv);
+    add_visc_flux(ff, uu, rv, g, dim, s.gr.ny > 1, s.gr.nz > 1, a.maxvel);
+  }
+  return E_OK;
+}
+__global__ void __launch_bounds__(128) k_face_flux(DevState s, DevScalars* sc, FluxArgs a, int dim) {
+  long n = dim == 0 ? s.gr.nx : dim == 1 ? s.gr.ny : s.gr.nz;
+  int c0d = dim == 0 ? 1 : 0, c1d = dim == 2 ? 1 : 2;
+  long dims[3] = {s.gr.nx, s.gr.ny, s.gr.nz};
+  long lo0 = dims[c0d] > 1 ? -1 : 0, n0 = dims[c0d] > 1 ? dims[c0d] + 2 : dims[c0d];
+  long lo1 = dims[c1d] > 1 ? -1 : 0, n1 = dims[c1d] > 1 ? dims[c1d] + 2 : dims[c1d];
+  // thread x walks the x index: for dim 0 that is the face index
+  long nf0 = dim == 0 ? n + 1 : n0;
+  long nfo = dim == 0 ? n0 : n + 1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf0 * nfo * n1) return;
+  long a0 = t % nf0, q = t / nf0;
+  long a1 = q % nfo, a2 = q / nfo;
+  long f, cx0, cx1;
+  if (dim == 0) {
+    f = a0;
+    cx0 = lo0 + a1;
+  } else {
+    cx0 = lo0 + a0;
+    f = a1;
+  }
+  cx1 = lo1 + a2;
+  long cf[3];
+  cf[dim] = f;
+  cf[c0d] = cx0;
+  cf[c1d] = cx1;
+  const Grid& g = s.gr.g;
+  long nc = s.gr.nc;
+  // stencil cells f-3 .. f+2 along dim
+  long cst[6];
+  for (int k = 0; k < 6; ++k) {
+    long cc[3] = {cf[0], cf[1], cf[2]};
+    cc[dim] = f - 3 + k;
+    cst[k] = cidx(s.gr, cc[0], cc[1], cc[2]);
+  }
+  double dxs[6];
+  for (int k = 0; k < 6; ++k) dxs[k] = cell_size(g, f - 3 + k, dim);
+  double pL[NV], pR[NV];
+  for (int iv = 0; iv < NV; ++iv) {
+    double v[6];
+    for (int k = 0; k < 6; ++k) v[k] = s.p[iv * nc + cst[k]];
+    Faces fl = reconstruct(RECON_PPM, v, dxs, a.theta);          // cell f-1: right face value
+    Faces fr = reconstruct(RECON_PPM, v + 1, dxs + 1, a.theta);  // cell f: left face value
+    pL[iv] = fl.right;
+    pR[iv] = fr.left;
+  }
+  Geom geo;
+  geom_face(s, cf[0], cf[1], cf[2], dim, geo);
+  long c = cst[3], cm = cst[2];
+  double ffl[NV], ffr[NV], uL[NV], uR[NV];
+  int e = face_state(s, sc, a, dim, pL, geo, c, cm, ffl, uL);
+  if (!e) e = face_state(s, sc, a, dim, pR, geo, c, cm, ffr, uR);
+  if (e) {
+    set_err(sc, e, c);
+    return;
+  }
+  double ag = kmath::fmax(s.amax[(long)dim * nc + c], s.amax[(long)dim * nc + cm]);
+  double agr = kmath::fmax(s.amax[(long)(3 + dim) * nc + c], s.amax[(long)(3 + dim) * nc + cm]);
+  long fi = face_index(s.gr, dim, cf[0], cf[1], cf[2]);
+  double* out = s.flb[dim];
+  long nfd = s.nf[dim];
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) out[iv * nfd + fi] = laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
+}
+
+// ---- flux-CT (koral/sim/ct.zig:38) --------------------------------------------
+__device__ __forceinline__ long pin(long n, long i) { return n == 1 ? 0 : i; }
+__device__ __forceinline__ double flbv(const DevState& s, int dim, int iv, long ix, long iy, long iz) {
+  return s.flb[dim][(long)iv * s.nf[dim] + face_index(s.gr, dim, ix, iy, iz)];
+}
+__global__ void k_ct_emf(DevState s) {
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (nx + 1) * (ny + 1) * (nz + 1)) return;
+  long ix = t % (nx + 1), q = t / (nx + 1), iy = q % (ny + 1), iz = q / (ny + 1);
+  double coef1 = (ny > 1 && nz > 1) ? 0.25 : 0.5;
+  double coef2 = (nx > 1 && nz > 1) ? 0.25 : 0.5;
+  double coef3 = (nx > 1 && ny > 1) ? 0.25 : 0.5;
+  if (ny > 1 || nz > 1) {
+    double sm = 0.0;
+    if (ny > 1) sm += flbv(s, 1, B3, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 1, B3, pin(nx, ix), pin(ny, iy), pin(nz, iz - 1));
+    if (nz > 1) sm -= flbv(s, 2, B2, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 2, B2, pin(nx, ix), pin(ny, iy - 1), pin(nz, iz));
+    s.emf[0][t] = coef1 * sm;
+  } else {
+    s.emf[0][t] = 0.0;
+  }
+  if (nx > 1 || nz > 1) {
+    double sm = 0.0;
+    if (nz > 1) sm += flbv(s, 2, B1, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 2, B1, pin(nx, ix - 1), pin(ny, iy), pin(nz, iz));
+    if (nx > 1) sm -= flbv(s, 0, B3, ix, pin(ny, iy), pin(nz, iz)) + flbv(s, 0, B3, ix, pin(ny, iy), pin(nz, iz - 1));
+    s.emf[1][t] = coef2 * sm;
+  } else {
+    s.emf[1][t] = 0.0;
+  }
+  if (nx > 1 || ny > 1) {
+    double sm = 0.0;
+    if (nx > 1) sm += flbv(s, 0, B2, ix, pin(ny, iy), pin(nz, iz)) + flbv(s, 0, B2, ix, pin(ny, iy - 1), pin(nz, iz));
+    if (ny > 1) sm -= flbv(s, 1, B1, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 1, B1, pin(nx, ix - 1), pin(ny, iy), pin(nz, iz));
+    s.emf[2][t] = coef3 * sm;
+  } else {
+    s.emf[2][t] = 0.0;
+  }
+}
+__global__ void k_ct_rebuild(DevState s) {
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (nx + 1) * (ny + 1) * (nz + 1)) return;
+  long ix = t % (nx + 1), q = t / (nx + 1), iy = q % (ny + 1), iz = q / (ny + 1);
+  auto E = [&](int comp, long jx, long jy, long jz) { return s.emf[comp - 1][(jz * (ny + 1) + jy) * (nx + 1) + jx]; };
+  if (nx > 1 && iy < ny && iz < nz) {
+    long fi = face_index(s.gr, 0, ix, iy, iz), nf = s.nf[0];
+    s.flb[0][B1 * nf + fi] = 0.0;
+    s.flb[0][B2 * nf + fi] = 0.5 * (E(3, ix, iy, iz) + E(3, ix, iy + 1, iz));
+    s.flb[0][B3 * nf + fi] = -0.5 * (E(2, ix, iy, iz) + E(2, ix, iy, iz + 1));
+  }
+  if (ny > 1 && ix < nx && iz < nz) {
+    long fi = face_index(s.gr, 1, ix, iy, iz), nf = s.nf[1];
+    s.flb[1][B1 * nf + fi] = -0.5 * (E(3, ix, iy, iz) + E(3, ix + 1, iy, iz));
+    s.flb[1][B2 * nf + fi] = 0.0;
+    s.flb[1][B3 * nf + fi] = 0.5 * (E(1, ix, iy, iz) + E(1, ix, iy, iz + 1));
+  }
+  if (nz > 1 && ix < nx && iy < ny) {
+    long fi = face_index(s.gr, 2, ix, iy, iz), nf = s.nf[2];
+    s.flb[2][B1 * nf + fi] = 0.5 * (E(2, ix, iy, iz) + E(2, ix + 1, iy, iz));
+    s.flb[2][B2 * nf + fi] = -0.5 * (E(1, ix, iy, iz) + E(1, ix, iy + 1, iz));
+    s.flb[2][B3 * nf + fi] = 0.0;
+  }
+}
+
+// ---- conserved update + metric source (sim.zig:1140,1542) --------------------
+__global__ void __launch_bounds__(128) k_update(DevState s, double gam, double dtin) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  const Grid& g = s.gr.g;
+  double pp[NV];
+  load_cell(s.p, nc, c, pp);
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  double gdetu = geo.gdet;
+  double ss[NV];
+  for (int i = 0; i < NV; ++i) ss[i] = 0.0;
+  double tij[4][4], tl[4][4], rup[4][4], rl[4][4];
+  calc_tij(pp, geo, gam, tij);
+  lower_second(tij, geo, tl);
+  calc_rij(pp, geo, rup);
+  lower_second(rup, geo, rl);
+  const int rows[4] = {UU, VX, VY, VZ}, rrows[4] = {EE, FX, FY, FZ};
+  for (int a = 0; a < 4; ++a)
+    for (int l = 0; l < 4; ++l)
+      for (int nu = 0; nu < 4; ++nu) {
+        double k = s.kr[(long)(l * 10 + sym10(nu, a)) * nc + c];
+        ss[rows[nu]] += gdetu * tl[a][l] * k;
+        ss[rrows[nu]] += gdetu * rl[a][l] * k;
+      }
+  double dx = cell_size(g, ix, 0), dy = cell_size(g, iy, 1), dz = cell_size(g, iz, 2);
+  double dt = dtin;
+  long fx0 = face_index(s.gr, 0, ix, iy, iz), fx1 = face_index(s.gr, 0, ix + 1, iy, iz);
+  long fy0 = face_index(s.gr, 1, ix, iy, iz), fy1 = face_index(s.gr, 1, ix, iy + 1, iz);
+  long fz0 = face_index(s.gr, 2, ix, iy, iz), fz1 = face_index(s.gr, 2, ix, iy, iz + 1);
+  for (int iv = 0; iv < NV; ++iv) {
+    double flxl = s.flb[0][iv * s.nf[0] + fx0], flxr = s.flb[0][iv * s.nf[0] + fx1];
+    double flyl = s.flb[1][iv * s.nf[1] + fy0], flyr = s.flb[1][iv * s.nf[1] + fy1];
+    double flzl = s.flb[2][iv * s.nf[2] + fz0], flzr = s.flb[2][iv * s.nf[2] + fz1];
+    double du = -(flxr - flxl) * dt / dx - (flyr - flyl) * dt / dy - (flzr - flzl) * dt / dz;
+    double uo = s.u[iv * nc + c];
+    s.u[iv * nc + c] = uo + du + ss[iv] * dt;
+  }
+}
+
+// ---- implicit operator (sim.zig:1715) ----------------------------------------
+struct ImplArgs {
+  double gam, dt;
+  RadParams rp;
+  OpacParams op;
+  ImplicitParams ip;
+  int polar_nc;
+};
+__global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, ImplArgs a) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  if (a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  double uu[NV], pp[NV];
+  load_cell(s.u, nc, c, uu);
+  load_cell(s.p, nc, c, pp);
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  ImplicitResult res = solve_implicit_lab(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip);
+  if (res.ok) {
+    store_cell(s.u, nc, c, uu);
+    store_cell(s.p, nc, c, pp);
+    s.flags[5 * nc + c] = 0;
+    atomicAdd(&sc->n_iters, (unsigned long long)res.iters);
+    atomicAdd(&sc->n_solves, 1ULL);
+  } else {
+    s.flags[5 * nc + c] = -1;
+    atomicAdd(&sc->n_fail, 1ULL);
+  }
+}
+
+// ---- radiative viscosity (koral/sim/rijvisc.zig:266) ---------------------------
+struct ViscArgs {
+  double gam, dt, rhor, alpha;
+  OpacParams op;
+};
+__global__ void __launch_bounds__(128) k_rijvisc(DevState s, ViscArgs a) {
+  long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
+  Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
+  int nout = (ix < 0 || ix >= nx) + (iy < 0 || iy >= ny) + (iz < 0 || iz >= nz);
+  if (nout >= 2) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  const Grid& g = s.gr.g;
+  double pp[NV];
+  load_cell(s.p, nc, c, pp);
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  // C calc_shear_lab (rijvisc.zig:39), RAD branch
+  double du[4][4], du2[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      du[i][j] = 0.0;
+      du2[i][j] = 0.0;
+    }
+  double ucon[4], ucov[4];
+  ucon_ucov_from_prims(pp[FX], pp[FY], pp[FZ], geo, ucon, ucov);
+  long nd[3] = {nx, ny, nz};
+  for (int idim = 1; idim < 4; ++idim) {
+    int dim = idim - 1;
+    if (nd[dim] <= 1) continue;
+    long cm[3] = {ix, iy, iz}, cp[3] = {ix, iy, iz};
+    cm[dim] -= 1;
+    cp[dim] += 1;
+    long ccm = cidx(s.gr, cm[0], cm[1], cm[2]), ccp = cidx(s.gr, cp[0], cp[1], cp[2]);
+    Geom gm, gp;
+    geom_cell(s, cm[0], cm[1], cm[2], gm);
+    geom_cell(s, cp[0], cp[1], cp[2], gp);
+    double umc[4], umv[4], upc[4], upv[4];
+    ucon_ucov_from_prims(s.p[FX * nc + ccm], s.p[FY * nc + ccm], s.p[FZ * nc + ccm], gm, umc, umv);
+    ucon_ucov_from_prims(s.p[FX * nc + ccp], s.p[FY * nc + ccp], s.p[FZ * nc + ccp], gp, upc, upv);
+    double xm = gm.xx[idim], xc = geo.xx[idim], xp = gp.xx[idim];
+    for (int i = 0; i < 4; ++i) {
+      double dc = (upv[i] - umv[i]) / (xp - xm);
+      double dr = (upv[i] - ucov[i]) / (xp - xc);
+      double dl = (ucov[i] - umv[i]) / (xc - xm);
+      double dc2 = (upc[i] - umc[i]) / (xp - xm);
+      double dr2 = (upc[i] - ucon[i]) / (xp - xc);
+      double dl2 = (ucon[i] - umc[i]) / (xc - xm);
+      if ((ix < 0 && iy == 0 && iz == 0 && idim != 1) || (iy < 0 && ix == 0 && iz == 0 && idim != 2) ||
+          (iz < 0 && ix == 0 && iy == 0 && idim != 3)) {
+        du[i][idim] = dr;
+        du2[i][idim] = dr2;
+      } else if ((ix < 0 && iy == ny - 1 && iz == nz - 1 && idim != 1) ||
+                 (iy < 0 && ix == nx - 1 && iz == nz - 1 && idim != 2) ||
+                 (iz < 0 && ix == nx - 1 && iy == ny - 1 && idim != 3)) {
+        du[i][idim] = dl;
+        du2[i][idim] = dl2;
+      } else if ((ix >= nx && iy == 0 && iz == 0 && idim != 1) || (iy >= ny && ix == 0 && iz == 0 && idim != 2) ||
+                 (iz >= nz && ix == 0 && iy == 0 && idim != 3)) {
+        du[i][idim] = dr;
+        du2[i][idim] = dr2;
+      } else if ((ix >= nx && iy == ny - 1 && iz == nz - 1 && idim != 1) ||
+                 (iy >= ny && ix == nx - 1 && iz == nz - 1 && idim != 2) ||
+                 (iz >= nz && ix == nx - 1 && iy == ny - 1 && idim != 3)) {
+        du[i][idim] = dl;
+        du2[i][idim] = dl2;
+      } else {
+        du[i][idim] = dc;
+        du2[i][idim] = dc2;
+      }
+    }
+  }
+  double k[64];
+  kr_block(s, c, k);
+  double sl[4][4], shear[4][4];
+  shear_from_gradients(du, du2, ucon, ucov, geo, k, sl);
+  raise_both(sl, geo, shear);
+  double chi = calc_chi_slim(pp, geo, a.gam, a.op);
+  double dx[3] = {cell_size(g, ix, 0) * kmath::sqrt(geo.gg[1][1]), cell_size(g, iy, 1) * kmath::sqrt(geo.gg[2][2]),
+                  cell_size(g, iz, 2) * kmath::sqrt(geo.gg[3][3])};
+  double mindx;
+  if (ny == 1 && nz == 1) mindx = dx[0];
+  else if (nz == 1) mindx = kmath::fmin(dx[0], dx[1]);
+  else if (ny == 1) mindx = kmath::fmin(dx[0], dx[2]);
+  else mindx = kmath::fmin(dx[0], kmath::fmin(dx[1], dx[2]));
+  double nu = visc_coeff(chi, mindx, s.blg[26L * nc + c], a.rhor, a.alpha, a.dt);
+  double rv[4][4];
+  rij_visc(nu, pp[EE], shear, geo, rv);
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) s.rijvisc[(long)(i * 4 + j) * nc + c] = rv[i][j];
+}
+
+// ---- mimic dynamo (koral/sim/dynamo.zig) --------------------------------------
+// per-radius density-weighted scale height, the reference's iy-outer / iz-inner
+// accumulation order kept (one thread per radial column)
+__global__ void k_scale_height(DevState s) {
+  long ix = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= s.gr.nx) return;
+  long nc = s.gr.nc;
+  double sigma = 0.0, sth = 0.0;
+  for (long iy = 0; iy < s.gr.ny; ++iy)
+    for (long iz = 0; iz < s.gr.nz; ++iz) {
+      long c = cidx(s.gr, ix, iy, iz);
+      double gd = s.cgc[10L * nc + c];
+      double th = s.blg[27L * nc + c];
+      double rho = s.p[RHO * nc + c];
+      double dth = KP_PI / 2.0 - th;
+      sigma += rho * gd;
+      sth += rho * gd * dth * dth;
+    }
+  s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
+}
+struct DynArgs {
+  double gam, dt, a, rhor, risco;
+  DynamoParams dp;
+};
+__global__ void __launch_bounds__(128) k_dynamo_delta_a(DevState s, DevScalars* sc, DynArgs a) {
+  long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
+  Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  s.dyn_a[c] = 0.0;
+  Geom geo, gbl;
+  geom_cell(s, ix, iy, iz, geo);
+  geom_bl(s, c, gbl);
+  double jac[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) jac[i][j] = s.jbl[(long)(i * 4 + j) * nc + c];
+  double pp[NV];
+  load_cell(s.p, nc, c, pp);
+  double angle, bsq;
+  int e = field_angle(geo, gbl, jac, pp, angle, bsq);
+  if (e) {
+    set_err(sc, e, c);
+    return;
+  }
+  double rr = gbl.xx[1], th = gbl.xx[2];
+  if (rr < 1.0001 * a.rhor) return;
+  double prermhd = (a.gam - 1.0) * pp[UU];
+  double ehat = -calc_ff_rtt(pp, geo, nullptr);
+  prermhd += ehat / 3.0;
+  long gix = ix < 0 ? 0 : (ix > s.gr.nx - 1 ? s.gr.nx - 1 : ix);
+  DynamoOut o = dynamo_delta_a(a.dp, a.a, a.dt, a.rhor, a.risco, rr, th, pp[B3], bsq, angle, prermhd, geo.gg[3][3],
+                               s.scaleth[gix]);
+  s.dyn_a[c] = o.aphi;
+  if (a.dp.dampbeta) s.p[B3 * nc + c] = o.bphi;
+}
+// corner-averaged A (ct.zig:224); src is a component-major [3][nc] field
+// (for the dynamo only component 2 is stored, components 0/1 are zero)
+__global__ void k_corner_avg_a(DevState s, const double* src, int comp_stride_zero) {
+  long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz, nc = s.gr.nc;
+  long mz = nz == 1 ? 1 : nz + 1, my = ny == 1 ? 1 : ny + 1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (nx + 1) * my * mz) return;
+  long ix = t % (nx + 1), q = t / (nx + 1), iy = q % my, iz = q / my;
+  for (int cc = 0; cc < 3; ++cc) {
+    auto S = [&](long jx, long jy, long jz) -> double {
+      if (comp_stride_zero && cc < 2) return 0.0;
+      long off = comp_stride_zero ? 0 : (long)cc * nc;
+      return src[off + cidx(s.gr, jx, jy, jz)];
+    };
+    double a;
+    if (ny == 1 && nz == 1) a = 1.0 / 2.0 * (S(ix, iy, iz) + S(ix - 1, iy, iz));
+    else if (ny > 1 && nz == 1) a = 1.0 / 4.0 * (S(ix, iy, iz) + S(ix, iy - 1, iz) + S(ix - 1, iy, iz) + S(ix - 1, iy - 1, iz));
+    else if (nz > 1 && ny == 1) a = 1.0 / 4.0 * (S(ix, iy, iz) + S(ix, iy, iz - 1) + S(ix - 1, iy, iz) + S(ix - 1, iy, iz - 1));
+    else
+      a = 1.0 / 8.0 *
+          (S(ix, iy, iz) + S(ix, iy - 1, iz) + S(ix - 1, iy, iz) + S(ix - 1, iy - 1, iz) + S(ix, iy, iz - 1) +
+           S(ix, iy - 1, iz - 1) + S(ix - 1, iy, iz - 1) + S(ix - 1, iy - 1, iz - 1));
+    s.vecpot[(long)cc * nc + cidx(s.gr, ix, iy, iz)] = a;
+  }
+}
+// curl of the corner A (ct.zig:282) into vecpot 3..5, then (mode 0) superpose on
+// the domain B and refresh the magnetic conserveds (dynamo.zig:420), or
+// (mode 1) overwrite B and all conserveds (calc_BfromA ifoverwrite, domain part)
+__global__ void __launch_bounds__(128) k_curl_apply(DevState s, double gam, int mode) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, nz = s.gr.nz;
+  const Grid& g = s.gr.g;
+  auto V = [&](int cc, long jx, long jy, long jz) { return s.vecpot[(long)cc * nc + cidx(s.gr, jx, jy, jz)]; };
+  double dA[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) dA[i][j] = 0.0;
+  if (nz == 1) {
+    for (int cc = 0; cc < 3; ++cc) {
+      dA[cc + 1][2] = -(V(cc, ix, iy, iz) - V(cc, ix, iy + 1, iz) + V(cc, ix + 1, iy, iz) - V(cc, ix + 1, iy + 1, iz)) /
+                      (2.0 * cell_size(g, iy, 1));
+      dA[cc + 1][1] = -(V(cc, ix, iy, iz) + V(cc, ix, iy + 1, iz) - V(cc, ix + 1, iy, iz) - V(cc, ix + 1, iy + 1, iz)) /
+                      (2.0 * cell_size(g, ix, 0));
+      dA[cc + 1][3] = 0.0;
+    }
+  } else {
+    for (int cc = 0; cc < 3; ++cc) {
+      dA[cc + 1][1] = (V(cc, ix + 1, iy, iz) - V(cc, ix, iy, iz) + V(cc, ix + 1, iy + 1, iz) - V(cc, ix, iy + 1, iz) +
+                       V(cc, ix + 1, iy, iz + 1) - V(cc, ix, iy, iz + 1) + V(cc, ix + 1, iy + 1, iz + 1) -
+                       V(cc, ix, iy + 1, iz + 1)) /
+                      (4.0 * cell_size(g, ix, 0));
+      dA[cc + 1][2] = (V(cc, ix, iy + 1, iz) - V(cc, ix, iy, iz) + V(cc, ix + 1, iy + 1, iz) - V(cc, ix + 1, iy, iz) +
+                       V(cc, ix, iy + 1, iz + 1) - V(cc, ix, iy, iz + 1) + V(cc, ix + 1, iy + 1, iz + 1) -
+                       V(cc, ix + 1, iy, iz + 1)) /
+                      (4.0 * cell_size(g, iy, 1));
+      dA[cc + 1][3] = (V(cc, ix, iy, iz + 1) - V(cc, ix, iy, iz) + V(cc, ix + 1, iy, iz + 1) - V(cc, ix + 1, iy, iz) +
+                       V(cc, ix, iy + 1, iz + 1) - V(cc, ix, iy + 1, iz) + V(cc, ix + 1, iy + 1, iz + 1) -
+                       V(cc, ix + 1, iy + 1, iz)) /
+                      (4.0 * cell_size(g, iz, 2));
+    }
+  }
+  long c = cidx(s.gr, ix, iy, iz);
+  double gdet = s.cgc[10L * nc + c];
+  double b1 = (dA[2][3] - dA[3][2]) / gdet;
+  double b2 = (dA[3][1] - dA[1][3]) / gdet;
+  double b3 = (dA[1][2] - dA[2][1]) / gdet;
+  double pp[NV];
+  load_cell(s.p, nc, c, pp);
+  if (mode == 0) {
+    pp[B1] += b1;
+    pp[B2] += b2;
+    pp[B3] += b3;
+  } else {
+    pp[B1] = b1;
+    pp[B2] = b2;
+    pp[B3] = b3;
+  }
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  double uu[NV];
+  p2u(pp, uu, geo, gam);
+  s.p[B1 * nc + c] = pp[B1];
+  s.p[B2 * nc + c] = pp[B2];
+  s.p[B3 * nc + c] = pp[B3];
+  if (mode == 0) {
+    s.u[B1 * nc + c] = uu[B1];
+    s.u[B2 * nc + c] = uu[B2];
+    s.u[B3 * nc + c] = uu[B3];
+  } else {
+    store_cell(s.u, nc, c, uu);
+  }
+}
+
+}  // namespace kc

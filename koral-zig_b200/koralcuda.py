@@ -1,0 +1,276 @@
+"""Python host mirror of the engine's C ABI (include/koralcuda.h).
+
+`Sim` mirrors the reference's `Sim(cfg)` surface (koral/sim.zig:93): init,
+step(forced_dt), cflDt, setBc, calcU2p, initTimestepGuess, finishInit, and the
+p / u / flags fields in the reference's AoS layout (koral/field.zig:1-10),
+so a test written against the reference reads the same here. All compute
+runs in libkoralcuda.so on the GPU; there is no CPU path — constructing a
+Sim without the library or a CUDA device raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkoralcuda.so")
+NV = 13
+NFLAGS = 6
+
+KC_OK = 0
+KC_ERR_INVALID_CONFIG = 1
+KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
+KC_PLAIN_FP64, KC_MIXED = 0, 1
+KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING = 0, 1
+
+
+class KcGrid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("ng", ctypes.c_int32),
+                ("minx", ctypes.c_double), ("maxx", ctypes.c_double), ("miny", ctypes.c_double),
+                ("maxy", ctypes.c_double), ("minz", ctypes.c_double), ("maxz", ctypes.c_double)]
+
+
+_d, _i = ctypes.c_double, ctypes.c_int32
+
+
+class KcOptions(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", _i), ("bhspin", _d), ("mksr0", _d), ("mksh0", _d), ("mass", _d), ("gam", _d),
+        ("tsteplim", _d), ("minmod_theta", _d), ("rhofloor", _d), ("uurhoratiomin", _d), ("uurhoratiomax", _d),
+        ("b2rhoratiomax", _d), ("b2uuratiomax", _d), ("gammamaxhd", _d), ("isentropic_b2rhofloors", _i),
+        ("b2uufloor", _i), ("horizon_x1", _d), ("gammamaxrad", _d), ("eradfloor", _d), ("eerhoratiomin", _d),
+        ("eerhoratiomax", _d), ("eeuuratiomin", _d), ("eeuuratiomax", _d), ("bremsstrahlung", _i),
+        ("synchrotron", _i), ("kleinnishina", _i), ("comptonization", _i), ("synchrotron_bridge", _i),
+        ("scattering", _i), ("hfrac", _d), ("hefrac", _d), ("mu_gas", _d), ("mu_i", _d), ("mu_e", _d),
+        ("radimp_conv", _d), ("radimp_entrconv", _d), ("radimp_eps", _d), ("radimp_maxiter", _i),
+        ("radimp_convrel", _d), ("radimp_convrelerr", _d), ("radimp_convrelentr", _d),
+        ("radimp_convrelentrerr", _d), ("radimp_damping_factor", _d), ("radimp_max_en_change_down", _d),
+        ("radimp_max_en_change_up", _d), ("radimp_max_damping", _d), ("radimp_max_tgas_change", _d),
+        ("radimp_max_trad_change", _d), ("radimp_threshold", _d), ("radimp_start_with_bisect", _i),
+        ("radimp_scale_jacobian", _i), ("radimp_allow_rad_ceiling", _i), ("radimp_allow_entr_in_4dprim", _i),
+        ("radimp_opdamp_maxlevels", _i), ("radimp_opdamp_factor", _d), ("radimp_lag_opac", _i),
+        ("do_fixups", _i), ("do_u2prad_fixups", _i), ("do_radimp_fixups", _i), ("correct_polaraxis", _i),
+        ("nccorrectpolar", _i), ("radviscosity", _i), ("alpharadvisc", _d), ("maxradviscvel", _d), ("dynamo", _i),
+        ("alphadynamo", _d), ("thetaangle", _d), ("alphabeta", _d), ("betasaturated", _d), ("expectedhr", _d),
+        ("alphaflipssign", _i), ("dampbeta", _i), ("calchronthego", _i), ("reduceorderatbh", _i),
+        ("reduceorderafterfixup", _i), ("dampradwavespeednearaxis", _i), ("bc_x", _i), ("bc_y", _i), ("bc_z", _i),
+        ("precision", _i), ("implicit_mode", _i), ("device", _i)]
+
+
+class KcCounters(ctypes.Structure):
+    _fields_ = [("t", _d), ("dt", _d), ("own_dt", _d), ("tstepdenmax", _d), ("tstepdenmin", _d),
+                ("nstep", ctypes.c_int64), ("n_radimp_failures", ctypes.c_int64),
+                ("n_radimp_fail_step", ctypes.c_int64), ("n_radimp_iters", ctypes.c_int64),
+                ("n_radimp_solves", ctypes.c_int64), ("n_guard_recoveries", ctypes.c_int64)]
+
+
+class KcStepInfo(ctypes.Structure):
+    _fields_ = [("dt", _d), ("nan_cell", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libkoralcuda.so (built in-tree by `make -C koral-zig_b200`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libkoralcuda.so is not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    P = ctypes.POINTER
+    L.kc_options_puffy.argtypes = [P(KcOptions)]
+    L.kc_options_puffy.restype = None
+    L.kc_grid_puffy.argtypes = [i32, i32, i32, P(KcGrid)]
+    L.kc_grid_puffy.restype = None
+    L.kc_create.argtypes = [P(KcGrid), P(KcOptions), P(vp)]
+    L.kc_destroy.argtypes = [vp]
+    L.kc_destroy.restype = None
+    L.kc_last_error.argtypes = [vp]
+    L.kc_last_error.restype = ctypes.c_char_p
+    for n in ["kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons", "kc_upload_flags",
+              "kc_download_flags"]:
+        getattr(L, n).argtypes = [vp, vp]
+    L.kc_set_counters.argtypes = [vp, P(KcCounters)]
+    L.kc_get_counters.argtypes = [vp, P(KcCounters)]
+    for n in ["kc_finish_init", "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p"]:
+        getattr(L, n).argtypes = [vp]
+    L.kc_cfl_dt.argtypes = [vp, P(dbl)]
+    L.kc_step.argtypes = [vp, dbl, P(KcStepInfo)]
+    L.kc_step_n.argtypes = [vp, i32, dbl]
+    L.kc_set_precision.argtypes = [vp, i32]
+    L.kc_set_implicit_mode.argtypes = [vp, i32]
+    L.kc_set_guess.argtypes = [vp, i32, vp, i64]
+    L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64]
+    L.kc_implicit_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
+    L.kc_u2p_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp]
+    L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
+    L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
+    for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
+              "kc_upload_flags", "kc_download_flags", "kc_set_counters", "kc_get_counters", "kc_finish_init",
+              "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p", "kc_cfl_dt", "kc_step", "kc_step_n",
+              "kc_set_precision", "kc_set_implicit_mode", "kc_set_guess", "kc_init_puffy", "kc_implicit_batch",
+              "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array"]:
+        getattr(L, n).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def puffy_options(**overrides):
+    """Sim.Options of the PUFFY problem (koral/problems/puffy/puffy.zig:210)."""
+    o = KcOptions()
+    lib().kc_options_puffy(ctypes.byref(o))
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+def puffy_grid(nx, ny, nz=1):
+    """The PUFFY MKS2 grid (koral/problems/puffy/puffy.zig:185 makeGridNz)."""
+    g = KcGrid()
+    lib().kc_grid_puffy(nx, ny, nz, ctypes.byref(g))
+    return g
+
+
+class KoralError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"status {status}: {msg}")
+        self.status = status
+
+
+class Sim:
+    """One engine instance: the device-resident state of the reference's Sim."""
+
+    def __init__(self, grid, opt):
+        self._lib = lib()
+        self._h = ctypes.c_void_p()
+        st = self._lib.kc_create(ctypes.byref(grid), ctypes.byref(opt), ctypes.byref(self._h))
+        if st != KC_OK:
+            msg = self._lib.kc_last_error(self._h).decode() if self._h else "kc_create failed"
+            self.close()
+            raise KoralError(st, msg)
+        self.grid = grid
+        sx = grid.nx + (2 * grid.ng if grid.nx > 1 else 0)
+        sy = grid.ny + (2 * grid.ng if grid.ny > 1 else 0)
+        sz = grid.nz + (2 * grid.ng if grid.nz > 1 else 0)
+        self.shape = (sz, sy, sx)
+        self.ncell = sx * sy * sz
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.kc_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, st):
+        if st != KC_OK:
+            raise KoralError(st, self._lib.kc_last_error(self._h).decode())
+
+    # ---- fields (koral/sim.zig:224-262) ---------------------------------------
+    def set_prims(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        assert p.size == self.ncell * NV
+        self._check(self._lib.kc_upload_prims(self._h, p.ctypes.data))
+
+    def set_cons(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.size == self.ncell * NV
+        self._check(self._lib.kc_upload_cons(self._h, u.ctypes.data))
+
+    def set_flags(self, f):
+        f = np.ascontiguousarray(f, dtype=np.int32)
+        assert f.size == self.ncell * NFLAGS
+        self._check(self._lib.kc_upload_flags(self._h, f.ctypes.data))
+
+    @property
+    def p(self):
+        out = np.empty((self.ncell, NV))
+        self._check(self._lib.kc_download_prims(self._h, out.ctypes.data))
+        return out
+
+    @property
+    def u(self):
+        out = np.empty((self.ncell, NV))
+        self._check(self._lib.kc_download_cons(self._h, out.ctypes.data))
+        return out
+
+    @property
+    def flags(self):
+        out = np.empty((self.ncell, NFLAGS), dtype=np.int32)
+        self._check(self._lib.kc_download_flags(self._h, out.ctypes.data))
+        return out
+
+    # ---- scalars (koral/sim.zig:237-293) --------------------------------------
+    def counters(self):
+        c = KcCounters()
+        self._check(self._lib.kc_get_counters(self._h, ctypes.byref(c)))
+        return {k: getattr(c, k) for k, _ in KcCounters._fields_}
+
+    def set_counters(self, **kw):
+        c = KcCounters()
+        self._check(self._lib.kc_get_counters(self._h, ctypes.byref(c)))
+        for k, v in kw.items():
+            setattr(c, k, v)
+        self._check(self._lib.kc_set_counters(self._h, ctypes.byref(c)))
+
+    # ---- methods (koral/sim.zig) -----------------------------------------------
+    def initTimestepGuess(self):
+        self._check(self._lib.kc_init_timestep_guess(self._h))
+
+    def finishInit(self):
+        self._check(self._lib.kc_finish_init(self._h))
+
+    def setBc(self):
+        self._check(self._lib.kc_set_bc(self._h))
+
+    def calcU2p(self):
+        self._check(self._lib.kc_calc_u2p(self._h))
+
+    def cflDt(self):
+        v = ctypes.c_double()
+        self._check(self._lib.kc_cfl_dt(self._h, ctypes.byref(v)))
+        return v.value
+
+    def step(self, forced_dt=None):
+        info = KcStepInfo()
+        dt = float("nan") if forced_dt is None else float(forced_dt)
+        self._check(self._lib.kc_step(self._h, dt, ctypes.byref(info)))
+        return info.dt
+
+    def initPuffy(self, perturb=0.0, perturb_rho=0.0, seed=0):
+        """puffy.initAllWith (koral/problems/puffy/puffy.zig:873) + initTimestepGuess."""
+        self._check(self._lib.kc_init_puffy(self._h, perturb, perturb_rho, seed))
+
+    def debug_phase(self, phase, dt=0.0):
+        self._check(self._lib.kc_debug_phase(self._h, phase, dt))
+
+
+def implicit_batch(opt, geom23, dt, pp, mode=KC_IMPLICIT_PER_CELL):
+    """solveImplicitLab over independent cells (koral/solve/implicit.zig:927)."""
+    geom23 = np.ascontiguousarray(geom23, dtype=np.float64)
+    dt = np.ascontiguousarray(dt, dtype=np.float64)
+    pp = np.array(pp, dtype=np.float64, order="C", copy=True)
+    n = pp.shape[0]
+    res = np.zeros((n, 6), dtype=np.int32)
+    st = lib().kc_implicit_batch(ctypes.byref(opt), n, geom23.ctypes.data, dt.ctypes.data, pp.ctypes.data,
+                                 res.ctypes.data, mode)
+    if st != KC_OK:
+        raise KoralError(st, "kc_implicit_batch")
+    return pp, res
+
+
+def u2p_batch(opt, geom23, uu, pp):
+    """The per-cell u2p cascade of calcU2p (koral/sim.zig:972-994)."""
+    geom23 = np.ascontiguousarray(geom23, dtype=np.float64)
+    uu = np.ascontiguousarray(uu, dtype=np.float64)
+    pp = np.array(pp, dtype=np.float64, order="C", copy=True)
+    n = pp.shape[0]
+    fl = np.zeros((n, 3), dtype=np.int32)
+    st = lib().kc_u2p_batch(ctypes.byref(opt), n, geom23.ctypes.data, uu.ctypes.data, pp.ctypes.data, fl.ctypes.data)
+    if st != KC_OK:
+        raise KoralError(st, "kc_u2p_batch")
+    return pp, fl

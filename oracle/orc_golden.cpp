@@ -63,6 +63,24 @@ extern "C" int orc_golden(const char* name, long nrec, const double* in, int nin
       for (int i = 0; i < NV; ++i) pp[i] = a[36 + i];
       o[10] = u2p_solver_w(a + 23, pp, g, ETYPE_ENTROPY, kGam);
       for (int i = 0; i < 9; ++i) o[11 + i] = pp[i];
+    } else if (!strcmp(name, "u2p_cascade")) {
+      // geom23 uu13 pp13 -> pp13 entropy_used hd_fixup rad_fixup: one cell of
+      // calcU2p's inversion (koral/sim.zig:972-994)
+      geom_from_record(a, 23, g);
+      double uu[NV], pp[NV];
+      for (int i = 0; i < NV; ++i) {
+        uu[i] = a[23 + i];
+        pp[i] = a[36 + i];
+      }
+      U2pMhdRes res = u2p_mhd(uu, pp, g, kGam, fl);
+      U2pRadRes rr = u2p_rad(uu, pp, g, rp);
+      int guards = 0;
+      check_floors_mhd(pp, g, kGam, fl, guards);
+      check_floors_rad(pp, g, rp);
+      for (int i = 0; i < NV; ++i) o[i] = pp[i];
+      o[13] = res.entropy_used;
+      o[14] = res.fixup;
+      o[15] = rr.corrected ? -1 : 0;
     } else if (!strcmp(name, "floors")) {
       geom_from_record(a, 23, g);
       double pp[NV];

@@ -12,46 +12,10 @@ NV = 13
 NFL = 6
 
 
-class KcGrid(ctypes.Structure):
-    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("ng", ctypes.c_int32),
-                ("minx", ctypes.c_double), ("maxx", ctypes.c_double), ("miny", ctypes.c_double),
-                ("maxy", ctypes.c_double), ("minz", ctypes.c_double), ("maxz", ctypes.c_double)]
+from tests.engine import koralcuda
 
-
-def _opt_fields():
-    d, i = ctypes.c_double, ctypes.c_int32
-    names = [
-        ("abi_version", i), ("bhspin", d), ("mksr0", d), ("mksh0", d), ("mass", d), ("gam", d), ("tsteplim", d),
-        ("minmod_theta", d), ("rhofloor", d), ("uurhoratiomin", d), ("uurhoratiomax", d), ("b2rhoratiomax", d),
-        ("b2uuratiomax", d), ("gammamaxhd", d), ("isentropic_b2rhofloors", i), ("b2uufloor", i), ("horizon_x1", d),
-        ("gammamaxrad", d), ("eradfloor", d), ("eerhoratiomin", d), ("eerhoratiomax", d), ("eeuuratiomin", d),
-        ("eeuuratiomax", d), ("bremsstrahlung", i), ("synchrotron", i), ("kleinnishina", i), ("comptonization", i),
-        ("synchrotron_bridge", i), ("scattering", i), ("hfrac", d), ("hefrac", d), ("mu_gas", d), ("mu_i", d),
-        ("mu_e", d), ("radimp_conv", d), ("radimp_entrconv", d), ("radimp_eps", d), ("radimp_maxiter", i),
-        ("radimp_convrel", d), ("radimp_convrelerr", d), ("radimp_convrelentr", d), ("radimp_convrelentrerr", d),
-        ("radimp_damping_factor", d), ("radimp_max_en_change_down", d), ("radimp_max_en_change_up", d),
-        ("radimp_max_damping", d), ("radimp_max_tgas_change", d), ("radimp_max_trad_change", d),
-        ("radimp_threshold", d), ("radimp_start_with_bisect", i), ("radimp_scale_jacobian", i),
-        ("radimp_allow_rad_ceiling", i), ("radimp_allow_entr_in_4dprim", i), ("radimp_opdamp_maxlevels", i),
-        ("radimp_opdamp_factor", d), ("radimp_lag_opac", i), ("do_fixups", i), ("do_u2prad_fixups", i),
-        ("do_radimp_fixups", i), ("correct_polaraxis", i), ("nccorrectpolar", i), ("radviscosity", i),
-        ("alpharadvisc", d), ("maxradviscvel", d), ("dynamo", i), ("alphadynamo", d), ("thetaangle", d),
-        ("alphabeta", d), ("betasaturated", d), ("expectedhr", d), ("alphaflipssign", i), ("dampbeta", i),
-        ("calchronthego", i), ("reduceorderatbh", i), ("reduceorderafterfixup", i), ("dampradwavespeednearaxis", i),
-        ("bc_x", i), ("bc_y", i), ("bc_z", i), ("precision", i), ("implicit_mode", i), ("device", i)]
-    return names
-
-
-class KcOptions(ctypes.Structure):
-    _fields_ = _opt_fields()
-
-
-class KcCounters(ctypes.Structure):
-    _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("own_dt", ctypes.c_double),
-                ("tstepdenmax", ctypes.c_double), ("tstepdenmin", ctypes.c_double), ("nstep", ctypes.c_int64),
-                ("n_radimp_failures", ctypes.c_int64), ("n_radimp_fail_step", ctypes.c_int64),
-                ("n_radimp_iters", ctypes.c_int64), ("n_radimp_solves", ctypes.c_int64),
-                ("n_guard_recoveries", ctypes.c_int64)]
+_kc = koralcuda()
+KcGrid, KcOptions, KcCounters = _kc.KcGrid, _kc.KcOptions, _kc.KcCounters
 
 
 _sim_bound = False

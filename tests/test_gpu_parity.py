@@ -1,0 +1,89 @@
+"""Parity of the sm_100a engine (libkoralcuda.so, through its C ABI) with the
+CPU oracle: the per-cell batch entry points on the reference's golden record
+inputs, and whole RK2IMEX steps from the reference's post-init self-golden
+states. The plain FP64 engine is built without FMA contraction and shares the
+oracle's per-point source, so every comparison here is bit for bit."""
+import numpy as np
+import pytest
+
+from tests.engine import koralcuda
+from tests.kgold import GOLDEN, load_kgld, run_golden
+from tests.orcsim import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+
+def _kc():
+    kc = koralcuda()
+    kc.lib()
+    return kc
+
+
+def test_implicit_batch_bitwise_on_golden_records():
+    kc = _kc()
+    i, _ = load_kgld("rad/rad_implicit")
+    z = run_golden("rad_implicit", i, 19)
+    pp, res = kc.implicit_batch(kc.puffy_options(), i[:, :23], i[:, 23], i[:, 24:37])
+    ok = res[:, 0] == 1
+    assert np.array_equal(ok, z[:, 0] == 0.0)
+    assert np.array_equal(res[ok, 3], z[ok, 1].astype(int))  # whichprim
+    assert np.array_equal(res[ok, 4], z[ok, 2].astype(int))  # whicheq
+    assert np.array_equal(res[ok, 2], z[ok, 4].astype(int))  # iterations
+    assert np.array_equal(res[:, 1], z[:, 18].astype(int))  # rung
+    assert np.array_equal(pp.view(np.uint64), z[:, 5:18].copy().view(np.uint64))
+
+
+def test_u2p_batch_bitwise_on_golden_records():
+    kc = _kc()
+    i, _ = load_kgld("state/u2p_solver")
+    geom, uu, guess = i[:, :23], i[:, 23:36], i[:, 36:49]
+    z = run_golden("u2p_cascade", np.concatenate([geom, uu, guess], axis=1), 16)
+    pp, fl = kc.u2p_batch(kc.puffy_options(), geom, uu, guess)
+    assert np.array_equal(pp.view(np.uint64), z[:, :13].copy().view(np.uint64))
+    assert np.array_equal(fl, z[:, 13:16].astype(np.int32))
+
+
+def _start(name):
+    kc = _kc()
+    z = np.load(f"{GOLDEN}/{name}_kslf.npz")
+    nx, ny = int(z["nx"]), int(z["ny"])
+    grid, opt = kc.puffy_grid(nx, ny), kc.puffy_options()
+    gpu = kc.Sim(grid, opt)
+    orc = OracleSim(grid, opt)
+    sc = z["scalars"][0]
+    for s in (gpu,):
+        s.set_prims(z["p"][0])
+        s.set_cons(z["u"][0])
+        s.set_flags(z["flags"][0])
+        s.initTimestepGuess()
+    orc.set_state(z["p"][0], z["u"][0], z["flags"][0])
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    assert gpu.counters()["tstepdenmax"] == orc.counters()["tstepdenmax"] == sc[3]
+    return z, gpu, orc
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.uint64)
+
+
+def _diff_report(a, b):
+    bad = np.nonzero(_bits(a) != _bits(b))
+    return f"{len(bad[0])} differing entries; first at {[x[:5] for x in bad]}"
+
+
+@pytest.mark.parametrize("nsteps", [1, 3])
+def test_step_bitwise_vs_oracle_puffy_fast(nsteps):
+    z, gpu, orc = _start("puffy_fast")
+    for _ in range(nsteps):
+        gpu.step()
+        orc.step()
+    cg, co = gpu.counters(), orc.counters()
+    for k in ["t", "dt", "own_dt", "tstepdenmax", "tstepdenmin"]:
+        assert cg[k] == co[k], (k, cg[k], co[k])
+    for k in ["n_radimp_failures", "n_radimp_iters", "n_radimp_solves", "n_guard_recoveries"]:
+        assert cg[k] == co[k], (k, cg[k], co[k])
+    pg, po = gpu.p, orc.prims()
+    assert np.array_equal(_bits(pg), _bits(po)), _diff_report(pg, po)
+    ug, uo = gpu.u, orc.cons()
+    assert np.array_equal(_bits(ug), _bits(uo)), _diff_report(ug, uo)
+    assert np.array_equal(gpu.flags, orc.flags())

@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Throughput of the full PUFFY GR-RMHD + M1 RK2IMEX step (koral/sim.zig:1792
+Sim.step) on the sm_100a engine, in zone-cycles/s (active cells x steps per
+second, the reference's `znps`, koral/problems/puffy/main.zig:99).
+
+Workload: the 3D wedge 192x180x64 MKS2 (periodic phi over +-pi/4, 3 ghost
+zones, NV=13), the PUFFY torus from the engine's own init with seeded 1e-3
+relative perturbations of u_int and rho, plain FP64. The state, metric cache
+and stage buffers (several GB) are far larger than the 126 MB L2, so no flush
+is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl koral|reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (the
+path does not shard in this tier); `value` is the whole job's zone-cycles
+over the slowest rank's device time. `--impl reference` times the CPU
+restatement of the same step (the oracle; the reference's Zig toolchain is
+not available) on all host cores, rank 0 only.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "zone-cycles/s (full GR-RMHD+M1 step)"
+UNIT = "zone-cycles/s"
+SAMPLE_NZ = 4  # phi cells of the CPU sample: same 192x180 meridional grid, 4 of the 64 phi cells
+
+# Algorithmic HBM bytes per cell and launch of each step pass (FP64, SoA, the
+# packed metric cache: center gcov10+gdet 11 f64, gcon16+gttpert 17 f64,
+# Christoffels 40 f64, BL geometry 28 f64; face metric 11+17 f64 per face).
+# Every cell's data counted once per launch; ghost/face overhangs ignored.
+B = 8
+PASS_BYTES_PER_CELL = {
+    # p, u in; p, u out; center metric 28; radimp flag
+    "implicit": (13 + 13 + 28 + 13 + 13) * B + 4,
+    # per active dim: p in, face metric 28, wavespeeds 6, rijvisc 16; flb out 13
+    "fluxes": None,  # dims-dependent, filled in by pass_bytes()
+    # u, p in; center metric 28; p out (5 MHD + 4 rad + ENTR), 6 flags out
+    "u2p": (13 + 13 + 28 + 13) * B + 6 * 4,
+    # flb in (13 per face and dim), u in/out, metric 28, Christoffels 40
+    "update": None,
+    # p, center metric 28, BL geometry 28, wavespeeds 6 + cell dt 2 out
+    "wavespeeds": (13 + 28 + 28 + 8) * B,
+    # p in, rijvisc 16 out, metric 28, BL radius
+    "radvisc": (13 + 28 + 16 + 1) * B,
+}
+
+
+def pass_bytes(name, ndim):
+    if name == "fluxes":
+        return ndim * (13 + 28 + 6 + 16 + 13) * B
+    if name == "update":
+        return (ndim * 13 + 13 + 13 + 28 + 40) * B
+    return PASS_BYTES_PER_CELL.get(name)
+
+
+def load_engine():
+    spec = importlib.util.spec_from_file_location("koralcuda", os.path.join(ROOT, "koral-zig_b200", "koralcuda.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mod.lib()
+    return mod
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def profiled_traffic(kernel):
+    """dram bytes per cell of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_cell:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while alive."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+    def __init__(self, device):
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ident = vis.split(",")[device] if vis else str(device)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", ident, "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        for line in self.out.read().splitlines():
+            cols = [c.strip() for c in line.split(",")]
+            if len(cols) < 9:
+                continue
+            try:
+                sm.append(float(cols[1]))
+                smax.append(float(cols[2]))
+            except ValueError:
+                continue
+            for name, v in zip(self.REASONS, cols[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.out.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def oracle_rate(nx, ny, nz, steps, warmup, threads, min_seconds=0.0):
+    """zone-cycles/s of the CPU restatement (oracle/orc_sim.cpp) on a
+    nx x ny x nz PUFFY wedge, after its own init and `warmup` steps."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    sys.path.insert(0, ROOT)
+    from tests.orcsim import OracleSim, puffy_grid, puffy_options
+
+    sim = OracleSim(puffy_grid(nx, ny, nz), puffy_options(), nthreads=threads)
+    sim.init_puffy(1e-3, 1e-3, 1)
+    sim.lib.orc_sim_init_timestep_guess(sim.h)
+    for _ in range(warmup):
+        sim.step()
+    n, t = 0, 0.0
+    while n < steps or t < min_seconds:
+        t0 = time.perf_counter()
+        sim.step()
+        t += time.perf_counter() - t0
+        n += 1
+    sim.close()
+    return nx * ny * nz * n / t, n, t
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nz = SAMPLE_NZ
+    rate, n, t = oracle_rate(args.nx, args.ny, nz, args.steps, args.warmup, threads)
+    sample = (f"{args.nx}x{args.ny}x{nz} of the {args.nx}x{args.ny}x{args.nz} wedge (same meridional grid, "
+              f"{nz} phi cells), {n} steps after {args.warmup} warm-up, oracle/orc_sim.cpp on {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (PUFFY torus init + seeded 1e-3 rho/u_int noise)",
+        "config": {"workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz} MKS2, plain FP64, CPU sample"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="koral", choices=["koral", "reference"])
+    ap.add_argument("--nx", type=int, default=192)
+    ap.add_argument("--ny", type=int, default=180)
+    ap.add_argument("--nz", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=20250)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device (the engine has no CPU path)")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+
+    kc = load_engine()
+    grid = kc.puffy_grid(args.nx, args.ny, args.nz)
+    opt = kc.puffy_options(device=local)
+    sim = kc.Sim(grid, opt)
+    ncell = args.nx * args.ny * args.nz
+    ndim = sum(1 for d in (args.nx, args.ny, args.nz) if d > 1)
+    t0 = time.perf_counter()
+    fac = sim.initPuffy(1e-3, 1e-3, args.seed)
+    init_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        sim.step()
+    stream = torch.cuda.ExternalStream(sim.stream())
+
+    # ---- device-resident timing (value) ------------------------------------------
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sim.set_pass_timing(True)
+    n0 = sim.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sim.step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = sim.launch_count() - n0
+    passes = sim.pass_times()
+    sim.set_pass_timing(False)
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ncell * args.steps * world / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI with host buffers (e2e) ---------------------
+    # Each step: pinned host p, u, flags -> device, Sim.step, device -> host; the
+    # drop-in contract of a host-resident Sim whose step runs on the GPU.
+    ke = args.e2e_steps if args.e2e_steps is not None else max(3, args.steps // 4)
+    nc = sim.ncell
+    hp = torch.empty((nc, kc.NV), dtype=torch.float64, pin_memory=True).numpy()
+    hu = torch.empty((nc, kc.NV), dtype=torch.float64, pin_memory=True).numpy()
+    hf = torch.empty((nc, kc.NFLAGS), dtype=torch.int32, pin_memory=True).numpy()
+    lib, h = kc.lib(), sim._h
+    for fn, buf in ((lib.kc_download_prims, hp), (lib.kc_download_cons, hu), (lib.kc_download_flags, hf)):
+        sim._check(fn(h, buf.ctypes.data))
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ke):
+        sim._check(lib.kc_upload_prims(h, hp.ctypes.data))
+        sim._check(lib.kc_upload_cons(h, hu.ctypes.data))
+        sim._check(lib.kc_upload_flags(h, hf.ctypes.data))
+        sim.step()
+        sim._check(lib.kc_download_prims(h, hp.ctypes.data))
+        sim._check(lib.kc_download_cons(h, hu.ctypes.data))
+        sim._check(lib.kc_download_flags(h, hf.ctypes.data))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ems = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e_bytes = hp.nbytes + hu.nbytes + hf.nbytes
+    e2e = {"value": ncell * ke * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": e2e_bytes,
+           "d2h_bytes_per_step": e2e_bytes, "steps": ke}
+
+    # ---- roofline of the dominant pass ---------------------------------------------
+    peaks, peak_kind = measured_peaks()
+    total = sum(v[0] for v in passes.values())
+    table = {}
+    for name, (pms, calls) in passes.items():
+        if calls == 0:
+            continue
+        entry = {"ms_per_step": pms / args.steps, "share": pms / total if total else 0.0, "calls_per_step": calls / args.steps}
+        bpc = pass_bytes(name, ndim)
+        if bpc is not None:
+            entry["gbs"] = bpc * ncell / (pms / calls / 1e3) / 1e9
+        table[name] = entry
+    dom = max((n for n in table if n != "step"), key=lambda n: table[n]["ms_per_step"])
+    dom_ms, dom_calls = passes[dom]
+    bpc = pass_bytes(dom, ndim)
+    kernel = {"implicit": "k_implicit", "fluxes": "k_face_flux", "u2p": "k_u2p", "update": "k_update",
+              "wavespeeds": "k_wavespeeds", "radvisc": "k_rijvisc"}.get(dom, dom)
+    achieved = bpc * ncell / (dom_ms / dom_calls / 1e3) / 1e9 if bpc else None
+    tr = profiled_traffic(kernel)
+    roofline = {
+        "bound": "hbm", "kernel": kernel, "pass": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
+        "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"] if achieved else None,
+        "traffic": tr * ncell if tr else None, "algorithmic_bytes": bpc * ncell if bpc else None,
+        "avg_launch_ms": dom_ms / dom_calls,
+        "passes": table,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (PUFFY torus from the engine's init + seeded 1e-3 rho/u_int noise)",
+        "config": {"workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz} MKS2 (periodic phi), plain FP64",
+                   "cells": ncell, "ghosts": 3, "precision": "plain FP64", "l2": "inputs larger than L2 (no flush)",
+                   "init_seconds": init_s, "beta_norm_factor": fac, "parallelism": f"replicas x{world}"},
+        "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, t = oracle_rate(args.nx, args.ny, SAMPLE_NZ, 1, 1, threads, min_seconds=10.0)
+        line["cpu_baseline"] = {
+            "value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{args.nx}x{args.ny}x{SAMPLE_NZ} slice of the wedge, {n} steps ({t:.1f} s) after 1 warm-up, "
+                      "oracle/orc_sim.cpp"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,28 @@ enum { KC_PLAIN_FP64 = 0, KC_MIXED = 1 };
 enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
 enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1 };
 
+/* Pass ids of the per-pass timers, the members of koral/sim/timers.zig:4
+ * Pass that the device step has. KC_PASS_FLUXES covers the reference's
+ * `sweep` and `fluxes` passes, which the engine fuses into one face kernel;
+ * KC_PASS_STEP is the untimed remainder of a step, as there. */
+enum {
+  KC_PASS_STEP = 0,
+  KC_PASS_RADVISC,
+  KC_PASS_IMPLICIT,
+  KC_PASS_U2P,
+  KC_PASS_FIXUP,
+  KC_PASS_BC,
+  KC_PASS_CORRECT,
+  KC_PASS_WAVESPEEDS,
+  KC_PASS_FLUXES,
+  KC_PASS_FLUXCT,
+  KC_PASS_UPDATE,
+  KC_PASS_DYNAMO,
+  KC_PASS_STAGE,
+  KC_PASS_ENTROPY,
+  KC_NPASS
+};
+
 /* koral/grid.zig:22 (Grid.init): internal-coordinate extents */
 typedef struct kc_grid {
   int32_t nx, ny, nz, ng;
@@ -134,11 +156,17 @@ int kc_download_flags(kc_handle* h, int32_t* flags);
 int kc_set_counters(kc_handle* h, const kc_counters* c);
 int kc_get_counters(kc_handle* h, kc_counters* c);
 
-/* PUFFY initial state: puffy.initAllWith (puffy.zig:873) — limotorus,
- * atmosphere, A_phi seed, B from A, beta normalization. perturb is the
- * relative u_int noise amplitude and seed mixes into the per-cell hash
- * (puffy.zig:696 perturbXi); pass 0 for the unperturbed reference init. */
-int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed);
+/* PUFFY initial state: puffy.initAllWith (koral/problems/puffy/puffy.zig:873)
+ * — limotorus, atmosphere, A_phi seed, set_bc, B from A, set_bc, beta
+ * normalization — followed by Sim.initTimestepGuess, as
+ * koral/problems/puffy/main.zig:304-305 does; t and the counters restart at 0.
+ * perturb is the relative u_int noise amplitude of puffy.zig:750 (Physics
+ * .perturb), perturb_rho the same for rho (no reference counterpart; 0 leaves
+ * the reference's init unchanged); seed is XORed into the x1 word of the
+ * per-cell hash (puffy.zig:696 perturbXi; 0 is the reference's field, rho uses
+ * seed ^ 0x5DEECE66D). fac_out (may be NULL) receives the normalization
+ * factor sqrt(maxbeta / max beta) that initAllWith returns. */
+int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed, double* fac_out);
 /* Sim.finishInit (koral/sim.zig:686): ghost fill from p, then the dt guess */
 int kc_finish_init(kc_handle* h);
 /* Sim.initTimestepGuess (koral/sim.zig:693) */
@@ -152,6 +180,21 @@ int kc_cfl_dt(kc_handle* h, double* dt);
 int kc_step(kc_handle* h, double forced_dt, kc_step_info* info);
 /* host buffers -> step(s) -> host buffers in one call */
 int kc_step_n(kc_handle* h, int32_t nsteps, double forced_dt);
+
+/* Sim.timers (koral/sim/timers.zig:41 PassTimers): per-pass self time of the
+ * steps taken while timing is on, measured on the device with CUDA events at
+ * every pass boundary of the handle's stream. kc_set_pass_timing resets the
+ * totals; kc_get_pass_times fills KC_NPASS entries of milliseconds and of
+ * pass calls (either pointer may be NULL). */
+int kc_set_pass_timing(kc_handle* h, int32_t on);
+int kc_get_pass_times(kc_handle* h, double* ms, int64_t* calls);
+const char* kc_pass_name(int32_t pass);
+/* The handle's CUDA stream (a cudaStream_t), on which every step kernel is
+ * launched, and the number of kernels the step passes have launched since
+ * kc_create (no reference counterpart: device plumbing for callers that time
+ * or order work against the engine). */
+int kc_get_stream(kc_handle* h, void** stream);
+int kc_get_launch_count(kc_handle* h, int64_t* n);
 
 /* Engine forms (no reference counterpart) */
 int kc_set_precision(kc_handle* h, int32_t mode);

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "kc_kernels.cuh"
+#include "../../include/koral/kinit.h"
 
 using namespace kp;
 using namespace kc;
@@ -55,6 +56,17 @@ struct kc_handle {
   // step scalars (koral/sim.zig:237-293)
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
+  // per-pass device time (koral/sim/timers.zig PassTimers), off by default:
+  // an event is recorded at every pass boundary, and the interval up to the
+  // next event belongs to the innermost pass open at the first (self time)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_pass;
+  int pass_stack[8] = {};
+  int pass_depth = 0;
+  double pass_ms[KC_NPASS] = {};
+  long long pass_calls[KC_NPASS] = {};
+  long long n_launch = 0;  // kernels launched by step passes since create
   long long nstep = 0, n_fail = 0, n_fail_step = 0, n_iters = 0, n_solves = 0, n_guard = 0;
   std::string err;
   int last_status = 0;
@@ -204,6 +216,45 @@ int build_cache(kc_handle* h) {
   return st;
 }
 
+// ---- pass timers -----------------------------------------------------------------
+void pass_mark(kc_handle* h) {
+  size_t i = h->ev_pass.size();
+  if (i == h->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    h->ev_pool.push_back(e);
+  }
+  cudaEventRecord(h->ev_pool[i], h->stream);
+  h->ev_pass.push_back(h->pass_depth ? h->pass_stack[h->pass_depth - 1] : -1);
+}
+struct PassScope {
+  kc_handle* h;
+  bool on;
+  PassScope(kc_handle* hh, int pass) : h(hh), on(hh->timing && hh->pass_depth < 8) {
+    if (!on) return;
+    h->pass_stack[h->pass_depth++] = pass;
+    h->pass_calls[pass] += 1;
+    pass_mark(h);
+  }
+  void end() {
+    if (!on) return;
+    on = false;
+    --h->pass_depth;
+    pass_mark(h);
+  }
+  ~PassScope() { end(); }
+};
+// after the stream has drained: fold the recorded intervals into the totals
+void pass_collect(kc_handle* h) {
+  for (size_t i = 0; i + 1 < h->ev_pass.size(); ++i) {
+    int p = h->ev_pass[i];
+    if (p < 0) continue;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, h->ev_pool[i], h->ev_pool[i + 1]) == cudaSuccess) h->pass_ms[p] += ms;
+  }
+  h->ev_pass.clear();
+}
+
 // ---- pass wrappers (one launch each) -----------------------------------------
 int sync_check(kc_handle* h, const char* what) {
   cudaError_t e = cudaGetLastError();
@@ -222,19 +273,34 @@ BcArgs bc_args(kc_handle* h) {
 
 // C set_bc (koral/sim/bc.zig:40)
 void launch_set_bc(kc_handle* h) {
+  PassScope ps(h, KC_PASS_BC);
   const DGrid& gr = h->gr;
   BcArgs a = bc_args(h);
   cudaStream_t st = h->stream;
-  if (gr.ngx > 0) k_bc_faces<<<nblk(2L * gr.ngx * gr.ny * gr.nz), TPB, 0, st>>>(h->ds, h->dsc, a, 0);
-  if (gr.ngy > 0) k_bc_faces<<<nblk(2L * gr.ngy * gr.nx * gr.nz), TPB, 0, st>>>(h->ds, h->dsc, a, 1);
-  if (gr.ngz > 0) k_bc_faces<<<nblk(2L * gr.ngz * gr.nx * gr.ny), TPB, 0, st>>>(h->ds, h->dsc, a, 2);
+  if (gr.ngx > 0) {
+    ++h->n_launch;
+    k_bc_faces<<<nblk(2L * gr.ngx * gr.ny * gr.nz), TPB, 0, st>>>(h->ds, h->dsc, a, 0);
+  }
+  if (gr.ngy > 0) {
+    ++h->n_launch;
+    k_bc_faces<<<nblk(2L * gr.ngy * gr.nx * gr.nz), TPB, 0, st>>>(h->ds, h->dsc, a, 1);
+  }
+  if (gr.ngz > 0) {
+    ++h->n_launch;
+    k_bc_faces<<<nblk(2L * gr.ngz * gr.nx * gr.ny), TPB, 0, st>>>(h->ds, h->dsc, a, 2);
+  }
   if (gr.ny > 1 && gr.nz == 1) {
+    ++h->n_launch;
     k_corners_2d<<<1, 32, 0, st>>>(h->ds, a);
   } else if (gr.nz > 1 && gr.ny > 1) {
     long ng = gr.ng;
+    ++h->n_launch;
     k_edge_tubes<<<nblk(4L * (gr.nz + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 0, 1, 2);
+    ++h->n_launch;
     k_edge_tubes<<<nblk(4L * (gr.ny + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 0, 2, 1);
+    ++h->n_launch;
     k_edge_tubes<<<nblk(4L * (gr.nx + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 1, 2, 0);
+    ++h->n_launch;
     k_corner_cubes<<<nblk(ng * ng * ng), TPB, 0, st>>>(h->ds, a.gam);
   }
 }
@@ -243,10 +309,15 @@ void launch_calc_u2p(kc_handle* h) {
   const DGrid& gr = h->gr;
   long ndom = (long)gr.nx * gr.ny * gr.nz;
   int pnc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
+  PassScope ps(h, KC_PASS_U2P);
   cudaMemsetAsync(&h->dsc->any_hd, 0, sizeof(int), h->stream);
+  ++h->n_launch;
   k_u2p<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, h->sp.fl, h->sp.rp, pnc);
   if (h->sp.do_fixups) {
+    PassScope pf(h, KC_PASS_FIXUP);
+    ++h->n_launch;
     k_fixup_hd<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, pnc);
+    ++h->n_launch;
     k_fixup_apply<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc);
   }
   launch_set_bc(h);
@@ -256,6 +327,8 @@ void launch_do_correct(kc_handle* h) {
   if (!h->sp.correct_polaraxis) return;
   const DGrid& gr = h->gr;
   int ncp = h->sp.nccorrectpolar;
+  PassScope ps(h, KC_PASS_CORRECT);
+  ++h->n_launch;
   k_polar_correct<<<nblk((long)gr.nx * gr.nz * 2 * ncp), TPB, 0, h->stream>>>(h->ds, h->sp.gam, ncp);
 }
 
@@ -268,6 +341,8 @@ void launch_implicit(kc_handle* h, double dtin) {
   a.op = h->sp.op;
   a.ip = h->sp.ip;
   a.polar_nc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
+  PassScope ps(h, KC_PASS_IMPLICIT);
+  ++h->n_launch;
   k_implicit<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
 }
 
@@ -278,7 +353,9 @@ void launch_wavespeeds(kc_handle* h) {
   a.tsteplim = h->sp.tsteplim;
   a.op = h->sp.op;
   a.damp_nc = h->sp.dampradwavespeednearaxis;
+  PassScope ps(h, KC_PASS_WAVESPEEDS);
   long n = (long)(gr.nx + 2 * (gr.nx > 1)) * (gr.ny + 2 * (gr.ny > 1)) * (gr.nz + 2 * (gr.nz > 1));
+  ++h->n_launch;
   k_wavespeeds<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
 }
 
@@ -291,6 +368,7 @@ void launch_face_fluxes(kc_handle* h) {
   a.fl = h->sp.fl;
   a.radvisc = h->sp.radviscosity;
   long dims[3] = {gr.nx, gr.ny, gr.nz};
+  PassScope ps(h, KC_PASS_FLUXES);
   for (int d = 0; d < 3; ++d) cudaMemsetAsync(h->ds.flb[d], 0, (size_t)NV * h->ds.nf[d] * 8, h->stream);
   for (int dim = 0; dim < 3; ++dim) {
     if (dims[dim] <= 1) continue;
@@ -298,6 +376,7 @@ void launch_face_fluxes(kc_handle* h) {
     long n0 = dims[c0] > 1 ? dims[c0] + 2 : dims[c0];
     long n1 = dims[c1] > 1 ? dims[c1] + 2 : dims[c1];
     long n = (dims[dim] + 1) * n0 * n1;
+    ++h->n_launch;
     k_face_flux<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
   }
 }
@@ -305,7 +384,10 @@ void launch_face_fluxes(kc_handle* h) {
 void launch_flux_ct(kc_handle* h) {
   const DGrid& gr = h->gr;
   long n = (long)(gr.nx + 1) * (gr.ny + 1) * (gr.nz + 1);
+  PassScope ps(h, KC_PASS_FLUXCT);
+  ++h->n_launch;
   k_ct_emf<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  ++h->n_launch;
   k_ct_rebuild<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
 }
 
@@ -314,12 +396,17 @@ void launch_op_explicit(kc_handle* h, double dtin) {
   launch_face_fluxes(h);
   launch_flux_ct(h);
   const DGrid& gr = h->gr;
-  k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dtin);
+  {
+    PassScope ps(h, KC_PASS_UPDATE);
+    ++h->n_launch;
+    k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dtin);
+  }
   launch_calc_u2p(h);
 }
 
 void launch_rijvisc(kc_handle* h, double global_dt) {
   const DGrid& gr = h->gr;
+  PassScope ps(h, KC_PASS_RADVISC);
   cudaMemsetAsync(h->ds.rijvisc, 0, (size_t)16 * gr.nc * 8, h->stream);
   ViscArgs a;
   a.gam = h->sp.gam;
@@ -328,11 +415,14 @@ void launch_rijvisc(kc_handle* h, double global_dt) {
   a.alpha = h->sp.alpharadvisc;
   a.op = h->sp.op;
   long n = (long)(gr.nx + 2 * (gr.nx > 1)) * (gr.ny + 2 * (gr.ny > 1)) * (gr.nz + 2 * (gr.nz > 1));
+  ++h->n_launch;
   k_rijvisc<<<nblk(n), TPB, 0, h->stream>>>(h->ds, a);
 }
 
 void launch_dynamo(kc_handle* h, double dt) {
   const DGrid& gr = h->gr;
+  PassScope ps(h, KC_PASS_DYNAMO);
+  ++h->n_launch;
   k_scale_height<<<nblk(gr.nx, 64), 64, 0, h->stream>>>(h->ds);
   launch_set_bc(h);
   DynArgs a;
@@ -343,23 +433,31 @@ void launch_dynamo(kc_handle* h, double dt) {
   a.risco = r_isco_bl(h->sp.mp.a);
   a.dp = h->sp.dp;
   long n = (long)(gr.nx + 2 * (gr.nx > 1)) * (gr.ny + 2 * (gr.ny > 1)) * (gr.nz + 2 * (gr.nz > 1));
+  ++h->n_launch;
   k_dynamo_delta_a<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
   long my = gr.ny == 1 ? 1 : gr.ny + 1, mz = gr.nz == 1 ? 1 : gr.nz + 1;
+  ++h->n_launch;
   k_corner_avg_a<<<nblk((long)(gr.nx + 1) * my * mz, 256), 256, 0, h->stream>>>(h->ds, h->ds.dyn_a, 1);
+  ++h->n_launch;
   k_curl_apply<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, 0);
   launch_calc_u2p(h);
 }
 
 void launch_stage_deriv(kc_handle* h, double* dst, const double* a, const double* b, double delta) {
   const DGrid& gr = h->gr;
+  PassScope ps(h, KC_PASS_STAGE);
+  ++h->n_launch;
   k_stage_deriv<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds, dst, a, b, delta);
 }
 void launch_stage_combine(kc_handle* h, double* dst, const double* a, double f1, const double* b, double f2,
                           const double* c) {
   const DGrid& gr = h->gr;
+  PassScope ps(h, KC_PASS_STAGE);
+  ++h->n_launch;
   k_stage_combine<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds, dst, a, f1, b, f2, c);
 }
 void copy_field(kc_handle* h, double* dst, const double* src) {
+  PassScope ps(h, KC_PASS_STAGE);
   cudaMemcpyAsync(dst, src, (size_t)NV * h->gr.nc * 8, cudaMemcpyDeviceToDevice, h->stream);
 }
 
@@ -408,6 +506,7 @@ int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
   long long fail0 = h->n_fail;
   h->tstepdenmax = -1.0;
   h->tstepdenmin = 1.0e50;
+  PassScope pstep(h, KC_PASS_STEP);
   reset_step_scalars(h);
   const double gam_imex = KP_GAM_IMEX;
   double* u = h->ds.u;
@@ -425,6 +524,8 @@ int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
   if (h->sp.dynamo) launch_dynamo(h, dt);
   {
     const DGrid& gr = h->gr;
+    PassScope ps(h, KC_PASS_STAGE);
+    ++h->n_launch;
     k_copy_entropy_count<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds);
   }
   launch_stage_deriv(h, h->dut1, u, h->ut1, dt);
@@ -450,11 +551,15 @@ int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
   launch_set_bc(h);
   {
     const DGrid& gr = h->gr;
+    PassScope ps(h, KC_PASS_ENTROPY);
+    ++h->n_launch;
     k_update_entropy<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam);
   }
+  pstep.end();
   int st = sync_check(h, "step launch");
   if (st) return st;
   st = collect_step_scalars(h, true);
+  if (h->timing) pass_collect(h);
   h->t = t + dt;
   h->n_fail_step = h->n_fail - fail0;
   h->nstep += 1;
@@ -559,6 +664,7 @@ int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
 void kc_destroy(kc_handle* h) {
   if (!h) return;
   for (void* p : h->allocs) cudaFree(p);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -683,6 +789,41 @@ int kc_step_n(kc_handle* h, int32_t nsteps, double forced_dt) {
 }
 
 // debugging surface for the parity tests: run one pass
+int kc_set_pass_timing(kc_handle* h, int32_t on) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (h->pass_depth) return fail(h, KC_ERR_INVALID_CONFIG, "pass timing changed inside a pass");
+  h->timing = on != 0;
+  h->ev_pass.clear();
+  for (int i = 0; i < KC_NPASS; ++i) {
+    h->pass_ms[i] = 0.0;
+    h->pass_calls[i] = 0;
+  }
+  return KC_OK;
+}
+int kc_get_pass_times(kc_handle* h, double* ms, int64_t* calls) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  for (int i = 0; i < KC_NPASS; ++i) {
+    if (ms) ms[i] = h->pass_ms[i];
+    if (calls) calls[i] = h->pass_calls[i];
+  }
+  return KC_OK;
+}
+const char* kc_pass_name(int32_t pass) {
+  static const char* names[KC_NPASS] = {"step",  "radvisc",    "implicit", "u2p",    "fixup",  "bc",    "correct",
+                                        "wavespeeds", "fluxes", "fluxct",   "update", "dynamo", "stage", "entropy"};
+  return (pass >= 0 && pass < KC_NPASS) ? names[pass] : "";
+}
+int kc_get_stream(kc_handle* h, void** stream) {
+  if (!h || !stream) return KC_ERR_INVALID_CONFIG;
+  *stream = (void*)h->stream;
+  return KC_OK;
+}
+int kc_get_launch_count(kc_handle* h, int64_t* n) {
+  if (!h || !n) return KC_ERR_INVALID_CONFIG;
+  *n = h->n_launch;
+  return KC_OK;
+}
+
 int kc_debug_phase(kc_handle* h, int phase, double dt) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   reset_step_scalars(h);
@@ -692,6 +833,7 @@ int kc_debug_phase(kc_handle* h, int phase, double dt) {
     case 2: launch_flux_ct(h); break;
     case 3: {
       const DGrid& gr = h->gr;
+      ++h->n_launch;
       k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dt);
       break;
     }
@@ -743,11 +885,84 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
   if (mode != KC_GUESS_PLAIN) return fail(h, KC_ERR_INVALID_CONFIG, "learned guess not built");
   return KC_OK;
 }
-int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed) {
-  (void)perturb;
-  (void)perturb_rho;
-  (void)seed;
-  return fail(h, KC_ERR_INVALID_CONFIG, "PUFFY init not built");
+// The PUFFY init sequence (puffy.zig:873 initAllWith, then initTimestepGuess as
+// problems/puffy/main.zig:304 does). The limotorus profile and the per-cell
+// primitives are built on the host (one torus solve per (x1, x2) column, the
+// cells of a column in parallel threads); set_bc, B from A, the second set_bc
+// and the beta normalization run on the device.
+int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed, double* fac_out) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  const DGrid& gr = h->gr;
+  const Grid& g = gr.g;
+  const long nc = gr.nc;
+  const MetricParams mp = h->sp.mp;
+  kcinit::PuffyPhysics ph;
+  ph.mass = h->opt.mass;
+  kcinit::TorusConsts tc = kcinit::torus_consts(mp.a, ph);
+  std::vector<double> hp((size_t)NV * nc, 0.0), hu((size_t)NV * nc, 0.0);
+  std::vector<int> errs((size_t)g.nx * g.ny, 0);
+  const double gam = h->sp.gam;
+  host_par(0, (long)g.nx * g.ny, [&](long k) {
+    long ix = k % g.nx, iy = k / g.nx;
+    Geom gb0;
+    geometry_bl_at(g, mp, ix, iy, 0, gb0);
+    kcinit::DsVels dv = kcinit::init_dsandvels(gb0.xx[1], gb0.xx[2], mp.a, tc, ph);
+    for (long iz = 0; iz < g.nz; ++iz) {
+      double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
+      Geom geo, gbl;
+      geometry_at(MKS2, mp, x, geo);
+      geometry_bl_at(g, mp, ix, iy, iz, gbl);
+      double jac[4][4];
+      double xbl[4] = {0.0, gbl.xx[1], gbl.xx[2], gbl.xx[3]};
+      dxdx(xbl, BL, MKS2, mp, jac);
+      long c = (ix + g.ngx) + (iy + g.ngy) * gr.sx + (iz + g.ngz) * gr.sx * gr.sy;
+      double* pp = &hp[(size_t)c * NV];
+      int e = kcinit::prep_init_cell(geo, gbl, jac, dv, h->sp, ph, perturb, perturb_rho, seed, pp);
+      if (e) {
+        errs[k] = e;
+        return;
+      }
+      pp[ENTR] = s_from_u(pp[RHO], pp[UU], gam);
+      p2u(pp, &hu[(size_t)c * NV], geo, gam);
+    }
+  });
+  for (int e : errs)
+    if (e) return fail(h, e, "PUFFY init: a torus cell failed its velocity conversion");
+  h->last_status = 0;
+  h->err.clear();
+  int st = cuda_check(h, cudaMemsetAsync(h->ds.flags, 0, 6L * nc * sizeof(int), h->stream), "init");
+  if (!st) st = cuda_check(h, cudaMemsetAsync(h->ds.vecpot, 0, 6L * nc * sizeof(double), h->stream), "init");
+  if (!st) st = upload_field(h, h->ds.p, hp.data(), NV);
+  if (!st) st = upload_field(h, h->ds.u, hu.data(), NV);
+  if (st) return st;
+  reset_step_scalars(h);
+  launch_set_bc(h);
+  long my = gr.ny == 1 ? 1 : gr.ny + 1, mz = gr.nz == 1 ? 1 : gr.nz + 1;
+  k_corner_avg_a<<<nblk((long)(gr.nx + 1) * my * mz, 256), 256, 0, h->stream>>>(h->ds, h->ds.p + (long)B1 * nc, 0);
+  k_curl_apply<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, gam, 1);
+  k_init_ghost_b<<<nblk(nc), TPB, 0, h->stream>>>(h->ds, gam);
+  launch_set_bc(h);
+  if ((st = sync_check(h, "init")) || (st = collect_step_scalars(h, false))) return st;
+  // postinit: global beta maximum, then B *= sqrt(maxbeta / maxb) over the domain
+  reset_step_scalars(h);
+  k_init_beta_max<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->dsc, gam);
+  DevScalars z;
+  st = cuda_check(h, cudaMemcpyAsync(&z, h->dsc, sizeof(z), cudaMemcpyDeviceToHost, h->stream), "init");
+  if (!st) st = cuda_check(h, cudaStreamSynchronize(h->stream), "init");
+  if (st) return st;
+  double maxb = 0.0;
+  if (z.tsd_max_bits) memcpy(&maxb, &z.tsd_max_bits, 8);
+  double fac = kmath::sqrt(ph.maxbeta / maxb);
+  k_init_beta_scale<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, gam, fac);
+  if ((st = sync_check(h, "init"))) return st;
+  if ((st = cuda_check(h, cudaStreamSynchronize(h->stream), "init"))) return st;
+  h->t = 0.0;
+  h->dt = 0.0;
+  h->own_dt = 0.0;
+  h->nstep = 0;
+  h->n_fail = h->n_fail_step = h->n_iters = h->n_solves = h->n_guard = 0;
+  if (fac_out) *fac_out = fac;
+  return kc_init_timestep_guess(h);
 }
 
 }  // extern "C"

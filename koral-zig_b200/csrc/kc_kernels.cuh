@@ -1096,4 +1096,78 @@ __global__ void __launch_bounds__(128) k_curl_apply(DevState s, double gam, int 
   }
 }
 
+// ---- PUFFY init passes (puffy.zig:873 initAll) -------------------------------
+// calc_BfromA's overwrite outside the domain (ct.zig:184): a ghost cell takes
+// the curl scratch there, which the curl never writes and which holds zeros,
+// and all its conserveds are refreshed.
+__global__ void __launch_bounds__(128) k_init_ghost_b(DevState s, double gam) {
+  long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nc = s.gr.nc;
+  if (c >= nc) return;
+  long ix = c % s.gr.sx - s.gr.ngx, iy = (c / s.gr.sx) % s.gr.sy - s.gr.ngy, iz = c / (s.gr.sx * s.gr.sy) - s.gr.ngz;
+  if (ix >= 0 && ix < s.gr.nx && iy >= 0 && iy < s.gr.ny && iz >= 0 && iz < s.gr.nz) return;
+  double pp[NV], uu[NV];
+  load_cell(s.p, nc, c, pp);
+  pp[B1] = 0.0;
+  pp[B2] = 0.0;
+  pp[B3] = 0.0;
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  p2u(pp, uu, geo, gam);
+  store_cell(s.p, nc, c, pp);
+  store_cell(s.u, nc, c, uu);
+}
+// postinit pass 1 (puffy.zig:939 betaMaxRows): the domain maximum of
+// p_mag / p_tot with p_tot = p_gas + Ehat/3, as ordered bits of a positive
+// double in sc->tsd_max_bits (the reference starts its max at 0, and a NaN
+// never wins a `>` comparison).
+__global__ void __launch_bounds__(128) k_init_beta_max(DevState s, DevScalars* sc, double gam) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  double v = 0.0;
+  if (range_cell(r, ix, iy, iz)) {
+    long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+    double pp[NV];
+    load_cell(s.p, nc, c, pp);
+    Geom geo;
+    geom_cell(s, ix, iy, iz, geo);
+    double ucon[4], ucov[4], bcon[4], bcov[4], bsq;
+    ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], geo, ucon, ucov);
+    double B[3] = {pp[B1], pp[B2], pp[B3]};
+    bcon_bcov_bsq(B, ucon, ucov, geo, bcon, bcov, bsq);
+    double pmag = bsq / 2.0;
+    double ptot = (gam - 1.0) * pp[UU];
+    ptot += -calc_ff_rtt(pp, geo, nullptr) / 3.0;
+    double q = pmag / ptot;
+    if (q > 0.0) v = q;
+  }
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffff, v, o));
+  __shared__ double smax[32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) smax[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, smax[w]);
+    if (m > 0.0) atomicMax(&sc->tsd_max_bits, dbits(m));
+  }
+}
+// postinit pass 2 (puffy.zig:984 betaScaleRows): B *= fac and p2u, domain only
+__global__ void __launch_bounds__(128) k_init_beta_scale(DevState s, double gam, double fac) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  double pp[NV], uu[NV];
+  load_cell(s.p, nc, c, pp);
+  pp[B1] *= fac;
+  pp[B2] *= fac;
+  pp[B3] *= fac;
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  p2u(pp, uu, geo, gam);
+  store_cell(s.p, nc, c, pp);
+  store_cell(s.u, nc, c, uu);
+}
+
 }  // namespace kc

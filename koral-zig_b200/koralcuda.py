@@ -22,6 +22,7 @@ KC_ERR_INVALID_CONFIG = 1
 KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
 KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING = 0, 1
+KC_NPASS = 14
 
 
 class KcGrid(ctypes.Structure):
@@ -103,16 +104,23 @@ def lib():
     L.kc_set_precision.argtypes = [vp, i32]
     L.kc_set_implicit_mode.argtypes = [vp, i32]
     L.kc_set_guess.argtypes = [vp, i32, vp, i64]
-    L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64]
+    L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64, P(dbl)]
     L.kc_implicit_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
     L.kc_u2p_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp]
+    L.kc_set_pass_timing.argtypes = [vp, i32]
+    L.kc_get_pass_times.argtypes = [vp, vp, vp]
+    L.kc_pass_name.argtypes = [i32]
+    L.kc_pass_name.restype = ctypes.c_char_p
+    L.kc_get_stream.argtypes = [vp, P(vp)]
+    L.kc_get_launch_count.argtypes = [vp, P(i64)]
     L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
     L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
     for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
               "kc_upload_flags", "kc_download_flags", "kc_set_counters", "kc_get_counters", "kc_finish_init",
               "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p", "kc_cfl_dt", "kc_step", "kc_step_n",
               "kc_set_precision", "kc_set_implicit_mode", "kc_set_guess", "kc_init_puffy", "kc_implicit_batch",
-              "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array"]:
+              "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
+              "kc_get_stream", "kc_get_launch_count"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -241,9 +249,34 @@ class Sim:
         self._check(self._lib.kc_step(self._h, dt, ctypes.byref(info)))
         return info.dt
 
+    # ---- pass timers (koral/sim/timers.zig) and device plumbing -----------------
+    def set_pass_timing(self, on):
+        self._check(self._lib.kc_set_pass_timing(self._h, 1 if on else 0))
+
+    def pass_times(self):
+        """{pass name: (milliseconds, calls)} of the steps taken while timing was on."""
+        ms = np.zeros(KC_NPASS)
+        calls = np.zeros(KC_NPASS, dtype=np.int64)
+        self._check(self._lib.kc_get_pass_times(self._h, ms.ctypes.data, calls.ctypes.data))
+        return {self._lib.kc_pass_name(i).decode(): (float(ms[i]), int(calls[i])) for i in range(KC_NPASS)}
+
+    def stream(self):
+        """The handle's cudaStream_t as an integer."""
+        v = ctypes.c_void_p()
+        self._check(self._lib.kc_get_stream(self._h, ctypes.byref(v)))
+        return v.value or 0
+
+    def launch_count(self):
+        v = ctypes.c_int64()
+        self._check(self._lib.kc_get_launch_count(self._h, ctypes.byref(v)))
+        return v.value
+
     def initPuffy(self, perturb=0.0, perturb_rho=0.0, seed=0):
-        """puffy.initAllWith (koral/problems/puffy/puffy.zig:873) + initTimestepGuess."""
-        self._check(self._lib.kc_init_puffy(self._h, perturb, perturb_rho, seed))
+        """puffy.initAllWith (koral/problems/puffy/puffy.zig:873) + initTimestepGuess;
+        returns the beta normalization factor."""
+        fac = ctypes.c_double(0.0)
+        self._check(self._lib.kc_init_puffy(self._h, perturb, perturb_rho, seed, ctypes.byref(fac)))
+        return fac.value
 
     def debug_phase(self, phase, dt=0.0):
         self._check(self._lib.kc_debug_phase(self._h, phase, dt))

@@ -17,9 +17,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <thread>
 #include <vector>
 
+#include "../include/koral/kinit.h"
 #include "../include/koral/kvisc.h"
 
 using namespace kp;
@@ -130,18 +132,20 @@ struct OSim {
   }
 };
 
+// rows handed out one at a time from an atomic ticket (the dynamic tiles of
+// koral/threading.zig:235), since implicit-solve cost varies ~17x across rows;
+// every row writes only its own cells, so results do not depend on the order
 template <class Fn>
 void par_for(int nthreads, long lo, long hi, Fn fn) {
   if (nthreads <= 1 || hi - lo < 2) {
     for (long i = lo; i < hi; ++i) fn(i);
     return;
   }
+  std::atomic<long> next(lo);
   std::vector<std::thread> th;
-  long n = hi - lo;
   for (int w = 0; w < nthreads; ++w) {
-    long a = lo + n * w / nthreads, b = lo + n * (w + 1) / nthreads;
-    th.emplace_back([=]() {
-      for (long i = a; i < b; ++i) fn(i);
+    th.emplace_back([&]() {
+      for (long i = next.fetch_add(1); i < hi; i = next.fetch_add(1)) fn(i);
     });
   }
   for (auto& x : th) x.join();
@@ -1394,6 +1398,93 @@ int step(OSim& s, double forced_dt) {
   return E_OK;
 }
 
+// ---- PUFFY initial state (puffy.zig:873 initAllWith) -------------------------
+// prepinit + p2u over the domain (puffy.zig:839), set_bc, calc_BfromA with
+// overwrite (ct.zig:184: every cell, ghosts get the zero scratch B), set_bc,
+// postinit (puffy.zig:892: global beta max over the domain, B scaled by
+// sqrt(maxbeta/maxb), ghosts keep their unscaled B). Returns the error code;
+// `fac` receives the beta normalization factor.
+int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, double& fac) {
+  const Grid& g = s.g;
+  kcinit::PuffyPhysics ph;
+  ph.mass = s.opt.mass;
+  const double a = s.sp.mp.a;
+  kcinit::TorusConsts tc = kcinit::torus_consts(a, ph);
+  std::vector<int> errs(g.ny, 0);
+  par_for(s.nthreads, 0, g.ny, [&](long iy) {
+    for (long ix = 0; ix < g.nx; ++ix) {
+      const Geom& gb0 = s.blg[s.ci(ix, iy, 0)];
+      kcinit::DsVels dv = kcinit::init_dsandvels(gb0.xx[1], gb0.xx[2], a, tc, ph);
+      for (long iz = 0; iz < g.nz; ++iz) {
+        Geom geo;
+        s.geom(ix, iy, iz, geo);
+        const Geom& gbl = s.blg[s.ci(ix, iy, iz)];
+        double jac[4][4];
+        double xbl[4] = {0.0, gbl.xx[1], gbl.xx[2], gbl.xx[3]};
+        dxdx(xbl, BL, MKS2, s.sp.mp, jac);
+        double pp[NV];
+        int e = kcinit::prep_init_cell(geo, gbl, jac, dv, s.sp, ph, perturb, perturb_rho, seed, pp);
+        if (e) {
+          errs[iy] = e;
+          continue;
+        }
+        pp[ENTR] = s_from_u(pp[RHO], pp[UU], s.sp.gam);
+        double* P = s.P(ix, iy, iz);
+        for (int i = 0; i < NV; ++i) P[i] = pp[i];
+        p2u(P, s.U(ix, iy, iz), geo, s.sp.gam);
+      }
+    }
+  });
+  for (int e : errs)
+    if (e) return e;
+  int e = set_bc(s);
+  if (e) return e;
+  std::fill(s.vecpot.begin(), s.vecpot.end(), 0.0);
+  curl_from_a(s, s.p, NV, B1);
+  for (long iz = -g.ngz; iz < g.nz + g.ngz; ++iz)
+    for (long iy = -g.ngy; iy < g.ny + g.ngy; ++iy)
+      for (long ix = -g.ngx; ix < g.nx + g.ngx; ++ix) {
+        double* pp = s.P(ix, iy, iz);
+        const double* v = &s.vecpot[s.ci(ix, iy, iz) * 6];
+        pp[B1] = v[3];
+        pp[B2] = v[4];
+        pp[B3] = v[5];
+        Geom geo;
+        s.geom(ix, iy, iz, geo);
+        p2u(pp, s.U(ix, iy, iz), geo, s.sp.gam);
+      }
+  if ((e = set_bc(s))) return e;
+  double maxb = 0.0;
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy)
+      for (long ix = 0; ix < g.nx; ++ix) {
+        const double* pp = s.P(ix, iy, iz);
+        Geom geo;
+        s.geom(ix, iy, iz, geo);
+        double ucon[4], ucov[4], bcon[4], bcov[4], bsq;
+        ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], geo, ucon, ucov);
+        double B[3] = {pp[B1], pp[B2], pp[B3]};
+        bcon_bcov_bsq(B, ucon, ucov, geo, bcon, bcov, bsq);
+        double pmag = bsq / 2.0;
+        double ptot = (s.sp.gam - 1.0) * pp[UU];
+        ptot += -calc_ff_rtt(pp, geo, nullptr) / 3.0;
+        if (pmag / ptot > maxb) maxb = pmag / ptot;
+      }
+  fac = kmath::sqrt(ph.maxbeta / maxb);
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy)
+      for (long ix = 0; ix < g.nx; ++ix) {
+        double* pp = s.P(ix, iy, iz);
+        pp[B1] *= fac;
+        pp[B2] *= fac;
+        pp[B3] *= fac;
+        Geom geo;
+        s.geom(ix, iy, iz, geo);
+        p2u(pp, s.U(ix, iy, iz), geo, s.sp.gam);
+      }
+  return E_OK;
+}
+
 }  // namespace
 
 // ---- ctypes surface ----------------------------------------------------------
@@ -1507,6 +1598,9 @@ void orc_sim_init_timestep_guess(void* h) { init_timestep_guess(*(OSim*)h); }
 int orc_sim_set_bc(void* h) { return set_bc(*(OSim*)h); }
 int orc_sim_calc_u2p(void* h) { return calc_u2p(*(OSim*)h); }
 int orc_sim_step(void* h, double forced_dt) { return step(*(OSim*)h, forced_dt); }
+int orc_sim_init_puffy(void* h, double perturb, double perturb_rho, unsigned long long seed, double* fac) {
+  return init_puffy(*(OSim*)h, perturb, perturb_rho, seed, *fac);
+}
 // single passes, for localizing engine-vs-oracle differences
 int orc_sim_phase(void* h, int phase, double dt) {
   OSim& s = *(OSim*)h;

@@ -32,7 +32,7 @@ KGLD = [
     "metric/metric_points.kgld", "metric/coco_dxdx.kgld", "metric/krzysie_grid.kgld",
 ]
 KSLF = ["puffy_fast.kslf", "puffy_full.kslf"]
-KSTP = ["step/puffy64.kstp.gz"]
+KSTP = ["step/puffy64.kstp.gz", "step/puffy3d.kstp.gz"]
 
 
 def read_maybe_gz(path):
@@ -84,7 +84,7 @@ def conv_kstp(src, dst):
     nu = ncell * nv
     np.savez_compressed(dst, nx=nx, ny=ny, nz=nz, nv=nv, t=vals[:, 0], dt=vals[:, 1],
                         u=vals[:, 2:2 + nu].reshape(nrec, ncell, nv), p=vals[:, 2 + nu:2 + 2 * nu].reshape(nrec, ncell, nv),
-                        flags=vals[:, 2 + 2 * nu:].reshape(nrec, nf, ncell).astype(np.int32))
+                        flags=vals[:, 2 + 2 * nu:].reshape(nrec, ncell, nf).astype(np.int32))
 
 
 def main(ref):

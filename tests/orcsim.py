@@ -50,6 +50,9 @@ def _bind():
     lib.orc_sim_phase.restype = ctypes.c_int
     lib.orc_sim_get_array.argtypes = [vp, ctypes.c_int, vp]
     lib.orc_sim_get_array.restype = ctypes.c_int
+    lib.orc_sim_init_puffy.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong,
+                                       ctypes.POINTER(ctypes.c_double)]
+    lib.orc_sim_init_puffy.restype = ctypes.c_int
     lib.orc_options_puffy.argtypes = [ctypes.POINTER(KcOptions)]
     lib.orc_grid_puffy.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(KcGrid)]
     _sim_bound = True
@@ -128,6 +131,15 @@ class OracleSim:
         rc = self.lib.orc_sim_step(self.h, forced_dt)
         if rc:
             raise RuntimeError(f"oracle step failed with status {rc}")
+
+    def init_puffy(self, perturb=0.0, perturb_rho=0.0, seed=0):
+        """The PUFFY init sequence (prepinit, set_bc, B from A, set_bc,
+        beta normalization); returns the normalization factor."""
+        fac = ctypes.c_double(0.0)
+        rc = self.lib.orc_sim_init_puffy(self.h, perturb, perturb_rho, seed, ctypes.byref(fac))
+        if rc:
+            raise RuntimeError(f"oracle init failed with status {rc}")
+        return fac.value
 
     def phase(self, which, dt=0.0):
         return self.lib.orc_sim_phase(self.h, which, dt)

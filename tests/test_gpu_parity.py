@@ -87,3 +87,73 @@ def test_step_bitwise_vs_oracle_puffy_fast(nsteps):
     ug, uo = gpu.u, orc.cons()
     assert np.array_equal(_bits(ug), _bits(uo)), _diff_report(ug, uo)
     assert np.array_equal(gpu.flags, orc.flags())
+
+
+def _pair(grid, opt):
+    kc = _kc()
+    return kc.Sim(grid, opt), OracleSim(grid, opt)
+
+
+def _assert_same_state(gpu, orc):
+    pg, po = gpu.p, orc.prims()
+    assert np.array_equal(_bits(pg), _bits(po)), _diff_report(pg, po)
+    ug, uo = gpu.u, orc.cons()
+    assert np.array_equal(_bits(ug), _bits(uo)), _diff_report(ug, uo)
+    assert np.array_equal(gpu.flags, orc.flags())
+
+
+def test_init_bitwise_vs_oracle_puffy_fast():
+    kc = _kc()
+    grid, opt = kc.puffy_grid(32, 30), kc.puffy_options()
+    gpu, orc = _pair(grid, opt)
+    fg = gpu.initPuffy()
+    fo = orc.init_puffy()
+    assert fg == fo
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    assert gpu.counters()["tstepdenmax"] == orc.counters()["tstepdenmax"]
+    _assert_same_state(gpu, orc)
+
+
+def test_init_perturbed_3d_then_steps_bitwise():
+    """The bench's workload shape in small: a 3D wedge with periodic phi, the
+    seeded 1e-3 u_int / rho perturbations, then CFL steps."""
+    kc = _kc()
+    grid, opt = kc.puffy_grid(24, 20, 8), kc.puffy_options()
+    gpu, orc = _pair(grid, opt)
+    fg = gpu.initPuffy(1e-3, 1e-3, 12345)
+    fo = orc.init_puffy(1e-3, 1e-3, 12345)
+    assert fg == fo
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    _assert_same_state(gpu, orc)
+    for _ in range(2):
+        gpu.step()
+        orc.step()
+    cg, co = gpu.counters(), orc.counters()
+    for k in ["t", "dt", "tstepdenmax", "tstepdenmin", "n_radimp_failures", "n_radimp_iters"]:
+        assert cg[k] == co[k], (k, cg[k], co[k])
+    _assert_same_state(gpu, orc)
+
+
+@pytest.mark.parametrize("name", ["puffy64", "puffy3d"])
+def test_forced_dt_steps_bitwise_from_c_state(name):
+    """C KORAL's post-init state of the forced-dt step goldens (64x60, and the
+    32x30x4 wedge), stepped with C's dt sequence on both sides."""
+    from tests.test_oracle_kstp import load_domain
+
+    kc = _kc()
+    z = np.load(f"{GOLDEN}/{name}_kstp.npz")
+    grid, opt = kc.puffy_grid(int(z["nx"]), int(z["ny"]), int(z["nz"])), kc.puffy_options()
+    gpu, orc = _pair(grid, opt)
+    load_domain(orc, grid, z, 0)
+    gpu.set_prims(orc.prims())
+    gpu.set_cons(orc.cons())
+    gpu.set_flags(orc.flags())
+    gpu.setBc()
+    assert orc.lib.orc_sim_set_bc(orc.h) == 0
+    gpu.initTimestepGuess()
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    for k in range(1, z["t"].shape[0]):
+        gpu.step(float(z["dt"][k]))
+        orc.step(float(z["dt"][k]))
+    assert gpu.counters()["n_radimp_iters"] == orc.counters()["n_radimp_iters"]
+    _assert_same_state(gpu, orc)

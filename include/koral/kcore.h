@@ -66,7 +66,7 @@ KC_HD void lower_vec(const double a1[4], const Geom& g, double a2[4]) {
   for (int i = 0; i < 4; ++i) a2[i] = t[i];
 }
 // T^mu nu -> T^mu_nu (koral/relele.zig:160, C indices_2221)
-KC_HD void lower_second(const double t1[4][4], const Geom& g, double t2[4][4]) {
+KC_HDM void lower_second(const double t1[4][4], const Geom& g, double t2[4][4]) {
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) {
       double s = 0.0;
@@ -83,7 +83,7 @@ KC_HD void lower_second_row(const double t1[4][4], const Geom& g, int row, doubl
   }
 }
 // T_mu nu -> T^mu nu (koral/relele.zig:127, C indices_1122)
-KC_HD void raise_both(const double t1[4][4], const Geom& g, double t2[4][4]) {
+KC_HDM void raise_both(const double t1[4][4], const Geom& g, double t2[4][4]) {
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) {
       double s = 0.0;
@@ -102,7 +102,7 @@ KC_HD void transform_vec(const double uin[4], const double a[4][4], double uout[
   for (int i = 0; i < 4; ++i) uout[i] = t[i];
 }
 // T2 = A A T1 (koral/relele.zig:205, C multiply22)
-KC_HD void transform_tensor(const double t1[4][4], const double a[4][4], double t2[4][4]) {
+KC_HDM void transform_tensor(const double t1[4][4], const double a[4][4], double t2[4][4]) {
   double t[4][4];
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) {
@@ -157,7 +157,7 @@ KC_HD void velr_to_vel4(const double uin[4], const Geom& g, double out[4]) {
   out[3] = o3;
 }
 // general contravariant conversion (koral/relele.zig:292, C conv_vels_core)
-KC_HD int convert(const double uin[4], int from, int to, const Geom& g, int utmode, double uout[4]) {
+KC_HDM int convert(const double uin[4], int from, int to, const Geom& g, int utmode, double uout[4]) {
   bool ut_known = utmode == TRUST_UT;
   if (from == to) {
     double t[4] = {uin[0], uin[1], uin[2], uin[3]};
@@ -210,7 +210,7 @@ KC_HD int convert(const double uin[4], int from, int to, const Geom& g, int utmo
 }
 
 // Gas u^mu, u_mu from the VELR primitives (koral/relele.zig:356, infallible)
-KC_HD void ucon_ucov_from_prims(double v1, double v2, double v3, const Geom& g, double ucon[4], double ucov[4]) {
+KC_HDM void ucon_ucov_from_prims(double v1, double v2, double v3, const Geom& g, double ucon[4], double ucov[4]) {
   double uin[4] = {0.0, v1, v2, v3};
   velr_to_vel4(uin, g, ucon);
   lower_vec(ucon, g, ucov);
@@ -243,7 +243,7 @@ KC_HD void bcon_from_4vel(const double B[3], const double ucon[4], const double 
   for (int j = 1; j < 4; ++j) bcon[j] = (B[j - 1] + b0 * ucon[j]) * inv_ut;
 }
 // b^mu, b_mu, b^2 (bfield.zig:47, C calc_bcon_bcov_bsq_from_4vel)
-KC_HD void bcon_bcov_bsq(const double B[3], const double ucon[4], const double ucov[4], const Geom& g,
+KC_HDM void bcon_bcov_bsq(const double B[3], const double ucon[4], const double ucov[4], const Geom& g,
                          double bcon[4], double bcov[4], double& bsq) {
   bcon_from_4vel(B, ucon, ucov, bcon);
   lower_vec(bcon, g, bcov);
@@ -257,14 +257,14 @@ KC_HD void big_bcon_from_4vel(const double bcon[4], const double ucon[4], double
 
 // ---- gas thermodynamics (koral/physics/hydro.zig) ---------------------------
 // S(rho, u) (hydro.zig:31, C calc_Sfromu, log form)
-KC_HD double s_from_u(double rho, double u, double gam) {
+KC_HDM double s_from_u(double rho, double u, double gam) {
   double gammam1 = gam - 1.0;
   double indexn = 1.0 / gammam1;
   double pre = gammam1 * u;
   return rho * kmath::log(kmath::pow(pre, indexn) / kmath::pow(rho, indexn + 1.0));
 }
 // inverse of s_from_u (hydro.zig:43, C calc_ufromS)
-KC_HD double u_from_s(double s, double rho, double gam) {
+KC_HDM double u_from_s(double s, double rho, double gam) {
   double gammam1 = gam - 1.0;
   double indexn = 1.0 / gammam1;
   return kmath::pow(kmath::pow(rho, indexn + 1.0) * kmath::exp(s / rho), gammam1) / gammam1;
@@ -282,7 +282,7 @@ KC_HD void tij_from_state(const double pp[NV], const Geom& g, double gam, const 
     for (int j = 0; j < 4; ++j) t[i][j] = eta * ucon[i] * ucon[j] + ptot * g.GG[i][j] - bcon[i] * bcon[j];
 }
 // hydro.zig:53
-KC_HD void calc_tij(const double pp[NV], const Geom& g, double gam, double t[4][4]) {
+KC_HDM void calc_tij(const double pp[NV], const Geom& g, double gam, double t[4][4]) {
   double ucon[4], ucov[4], bcon[4], bcov[4], bsq;
   ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], g, ucon, ucov);
   double B[3] = {pp[B1], pp[B2], pp[B3]};
@@ -306,7 +306,7 @@ KC_HD double calc_utp1(const double vcon[4], const Geom& g) {
 }
 
 // hydro + magnetic conserveds (p2u.zig:39, C p2u_mhd)
-KC_HD void p2u_mhd(const double pp[NV], double uu[NV], const Geom& g, double gam) {
+KC_HDM void p2u_mhd(const double pp[NV], double uu[NV], const Geom& g, double gam) {
   double gdetu = g.gdet;
   double rho = pp[RHO], ugas = pp[UU], s = pp[ENTR];
   double vcon[4] = {0.0, pp[VX], pp[VY], pp[VZ]};
@@ -341,7 +341,7 @@ KC_HD void p2u_mhd(const double pp[NV], double uu[NV], const Geom& g, double gam
 }
 
 // M1 radiative conserveds R^t_mu (p2u.zig:103, C p2u_rad)
-KC_HD void p2u_rad(const double pp[NV], double uu[NV], const Geom& g) {
+KC_HDM void p2u_rad(const double pp[NV], double uu[NV], const Geom& g) {
   double gdetu = g.gdet;
   const double four_third = 4.0 / 3.0, one_third = 1.0 / 3.0;
   double erf = pp[EE];
@@ -355,7 +355,7 @@ KC_HD void p2u_rad(const double pp[NV], double uu[NV], const Geom& g) {
 }
 
 // full conserved vector (p2u.zig:135, C p2u)
-KC_HD void p2u(const double pp[NV], double uu[NV], const Geom& g, double gam) {
+KC_HDM void p2u(const double pp[NV], double uu[NV], const Geom& g, double gam) {
   p2u_mhd(pp, uu, g, gam);
   p2u_rad(pp, uu, g);
 }

@@ -39,7 +39,7 @@ KC_HD double my_sign(double x) {
 }
 
 // 4x4 LU inversion with partial pivoting, no error path (implicit.zig:172)
-KC_HD void invert4(const double a_in[4][4], double inv[4][4]) {
+KC_HDM void invert4(const double a_in[4][4], double inv[4][4]) {
   double lu[4][4];
   int perm[4] = {0, 1, 2, 3};
   for (int i = 0; i < 4; ++i)
@@ -181,7 +181,7 @@ KC_HDN double implicit_residual(const double uu[NV], const double pp[NV], const 
 }
 
 // C f_implicit_1dprim_err (implicit.zig:431)
-KC_HD double f1d_err(double xxx, const double pp0[NV], double dtau, const Geom& g, double gam, const OpacParams& op,
+KC_HDM double f1d_err(double xxx, const double pp0[NV], double dtau, const Geom& g, double gam, const OpacParams& op,
                      int whichprim, double totenergy, double ratio) {
   double ugas, ehat;
   if (whichprim == PRIM_RAD) {

@@ -215,7 +215,7 @@ struct U2pMhdRes {
   bool fixup;
 };
 // MHD part of C's u2p cascade (invert.zig:422)
-KC_HD U2pMhdRes u2p_mhd(const double uu_in[NV], double pp[NV], const Geom& g, double pgamma, const FloorParams& fl) {
+KC_HDM U2pMhdRes u2p_mhd(const double uu_in[NV], double pp[NV], const Geom& g, double pgamma, const FloorParams& fl) {
   double uu[NV], ppbak[NV], ppmhd[NV];
   for (int i = 0; i < NV; ++i) {
     uu[i] = uu_in[i];
@@ -369,7 +369,7 @@ KC_HDN int check_floors_mhd(double pp[NV], const Geom& g, double pgamma, const F
 
 // ---- M1 radiation (koral/physics/radiation.zig) ----------------------------
 // R^mu nu of the M1 closure (radiation.zig:79, C calc_Rij_M1)
-KC_HD void calc_rij(const double pp[NV], const Geom& g, double rij[4][4]) {
+KC_HDM void calc_rij(const double pp[NV], const Geom& g, double rij[4][4]) {
   const double four_third = 4.0 / 3.0, one_third = 1.0 / 3.0;
   double erf = pp[EE];
   double vin[4] = {0.0, pp[FX], pp[FY], pp[FZ]};
@@ -379,7 +379,7 @@ KC_HD void calc_rij(const double pp[NV], const Geom& g, double rij[4][4]) {
     for (int j = 0; j < 4; ++j) rij[i][j] = four_third * erf * urf[i] * urf[j] + one_third * erf * g.GG[i][j];
 }
 // C calc_ff_Rtt (radiation.zig:104): rtt = -R^mu_nu u^nu u_mu; also gas ucon
-KC_HD double calc_ff_rtt(const double pp[NV], const Geom& g, double ucon_out[4]) {
+KC_HDM double calc_ff_rtt(const double pp[NV], const Geom& g, double ucon_out[4]) {
   double ucon[4], ucov[4];
   ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], g, ucon, ucov);
   double rij_uu[4][4], rij_ud[4][4];
@@ -395,7 +395,7 @@ KC_HD double calc_ff_rtt(const double pp[NV], const Geom& g, double ucon_out[4])
 
 // ---- M1 inversion (koral/solve/invert_rad.zig) -----------------------------
 // C get_m1closure_gammarel2 (invert_rad.zig:66)
-KC_HD double m1_gammarel2(const Geom& g, const double av[4]) {
+KC_HDM double m1_gammarel2(const Geom& g, const double av[4]) {
   const double gsl = 1.0 - 1e-10;
   double gn11 = g.GG[0][0], gn12 = g.GG[0][1], gn13 = g.GG[0][2], gn14 = g.GG[0][3];
   double gn22 = g.GG[1][1], gn23 = g.GG[1][2], gn24 = g.GG[1][3];
@@ -433,7 +433,7 @@ KC_HD double m1_gammarel2(const Geom& g, const double av[4]) {
   return gammarel2;
 }
 // C get_m1closure_gammarel2_cold (invert_rad.zig:136)
-KC_HD void m1_cold(const Geom& g, const double av_in[4], double gammarel2, double av[4], double& erf, double urfconrel[4]) {
+KC_HDM void m1_cold(const Geom& g, const double av_in[4], double gammarel2, double av[4], double& erf, double urfconrel[4]) {
   double gn11 = g.GG[0][0], gn12 = g.GG[0][1], gn13 = g.GG[0][2], gn14 = g.GG[0][3];
   double gn22 = g.GG[1][1], gn23 = g.GG[1][2], gn24 = g.GG[1][3];
   double gn33 = g.GG[2][2], gn34 = g.GG[2][3], gn44 = g.GG[3][3];
@@ -520,7 +520,7 @@ KC_HDN U2pRadRes u2p_rad(const double uu[NV], double pp[NV], const Geom& g, cons
 }
 
 // C check_floors_rad (invert_rad.zig:266)
-KC_HD int check_floors_rad(double pp[NV], const Geom& g, const RadParams& rp) {
+KC_HDM int check_floors_rad(double pp[NV], const Geom& g, const RadParams& rp) {
   int ret = 0;
   double ehat = -calc_ff_rtt(pp, g, nullptr);
   double eratio = pp[EE] / ehat;

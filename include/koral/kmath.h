@@ -38,6 +38,15 @@
 #define KC_HD inline
 #define KC_HDN inline
 #endif
+// Mid-size helpers (p2u, the M1 closure, boosts, opacities' thermodynamics,
+// the 4x4 inverse): inlined unless KC_SHARED_HELPERS is 1, which compiles
+// them as calls and so shrinks the code of the large solver kernels. Either
+// way the arithmetic is the same (no contraction), so results are identical.
+#if defined(KC_SHARED_HELPERS) && KC_SHARED_HELPERS
+#define KC_HDM KC_HDN
+#else
+#define KC_HDM KC_HD
+#endif
 
 namespace kmath {
 

@@ -75,7 +75,7 @@ struct Temps {
   double tgas, te, ti;
 };
 // C calc_PEQ_Teifrompp single-temperature branch (thermo.zig:188)
-KC_HD Temps temps_from_urho(const Consts& c, double uint_, double rho, double gam) {
+KC_HDM Temps temps_from_urho(const Consts& c, double uint_, double rho, double gam) {
   Temps t;
   t.tgas = t_from_urho(c, uint_, rho, gam);
   double te = t.tgas, ti = t.tgas;
@@ -289,21 +289,21 @@ KC_HD void normal_obs_concov(const Geom& g, double con[4], double cov[4]) {
   raise_vec(cov, g, con);
 }
 // C calc_Lorentz_lab2ff (frames.zig:77)
-KC_HD void lorentz_lab2ff(double v1, double v2, double v3, const Geom& g, double l[4][4]) {
+KC_HDM void lorentz_lab2ff(double v1, double v2, double v3, const Geom& g, double l[4][4]) {
   double ucon[4], ucov[4], wcon[4], wcov[4];
   ucon_ucov_from_prims(v1, v2, v3, g, ucon, ucov);
   normal_obs_concov(g, wcon, wcov);
   lorentz_from_pair(ucon, ucov, wcon, wcov, l);
 }
 // C calc_Lorentz_ff2lab (frames.zig:84)
-KC_HD void lorentz_ff2lab(double v1, double v2, double v3, const Geom& g, double l[4][4]) {
+KC_HDM void lorentz_ff2lab(double v1, double v2, double v3, const Geom& g, double l[4][4]) {
   double wcon[4], wcov[4], ucon[4], ucov[4];
   ucon_ucov_from_prims(v1, v2, v3, g, wcon, wcov);
   normal_obs_concov(g, ucon, ucov);
   lorentz_from_pair(ucon, ucov, wcon, wcov, l);
 }
 // A2 = alpha (L_lab2ff A1) (frames.zig:101, C boost2_lab2ff)
-KC_HD void boost2_lab2ff(const double a1[4], double v1, double v2, double v3, const Geom& g, double a2[4]) {
+KC_HDM void boost2_lab2ff(const double a1[4], double v1, double v2, double v3, const Geom& g, double a2[4]) {
   double l[4][4];
   lorentz_lab2ff(v1, v2, v3, g, l);
   transform_vec(a1, l, a2);
@@ -311,7 +311,7 @@ KC_HD void boost2_lab2ff(const double a1[4], double v1, double v2, double v3, co
   for (int i = 0; i < 4; ++i) a2[i] *= alpha;
 }
 // A2 = L_ff2lab (A1 / alpha) (frames.zig:108, C boost2_ff2lab)
-KC_HD void boost2_ff2lab(const double a1[4], double v1, double v2, double v3, const Geom& g, double a2[4]) {
+KC_HDM void boost2_ff2lab(const double a1[4], double v1, double v2, double v3, const Geom& g, double a2[4]) {
   double l[4][4];
   lorentz_ff2lab(v1, v2, v3, g, l);
   double alpha = kmath::sqrt(-1.0 / g.GG[0][0]);
@@ -320,7 +320,7 @@ KC_HD void boost2_ff2lab(const double a1[4], double v1, double v2, double v3, co
   transform_vec(at, l, a2);
 }
 // T2 = L L T1, no alpha (frames.zig:147, C boost22_ff2lab)
-KC_HD void boost22_ff2lab(const double t1[4][4], double v1, double v2, double v3, const Geom& g, double t2[4][4]) {
+KC_HDM void boost22_ff2lab(const double t1[4][4], double v1, double v2, double v3, const Geom& g, double t2[4][4]) {
   double l[4][4];
   lorentz_ff2lab(v1, v2, v3, g, l);
   transform_tensor(t1, l, t2);
@@ -334,7 +334,7 @@ KC_HD double compton_gi_coeff(const Consts& c, const RadState& st) {
 }
 // C calc_all_Gi_with_state thermal part (radforce.zig:432). full=false leaves
 // ff[1..3] zero and skips the boost (the solver path).
-KC_HD void calc_gi_from_state(const RadState& st, double v1, double v2, double v3, const Geom& g, const OpacParams& op,
+KC_HDM void calc_gi_from_state(const RadState& st, double v1, double v2, double v3, const Geom& g, const OpacParams& op,
                               bool full, double gi_ff[4], double gi_lab[4]) {
   const Consts& c = op.c;
   double b = c.sigma_rad_over_pi * st.te * st.te * st.te * st.te;

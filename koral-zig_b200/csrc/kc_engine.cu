@@ -423,7 +423,7 @@ void launch_dynamo(kc_handle* h, double dt) {
   const DGrid& gr = h->gr;
   PassScope ps(h, KC_PASS_DYNAMO);
   ++h->n_launch;
-  k_scale_height<<<nblk(gr.nx, 64), 64, 0, h->stream>>>(h->ds);
+  k_scale_height<<<nblk(gr.nx, SH_COLS), SH_WARPS * 32, 0, h->stream>>>(h->ds);
   launch_set_bc(h);
   DynArgs a;
   a.gam = h->sp.gam;

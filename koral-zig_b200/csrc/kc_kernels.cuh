@@ -949,22 +949,42 @@ __global__ void __launch_bounds__(128) k_rijvisc(DevState s, ViscArgs a) {
 // ---- mimic dynamo (koral/sim/dynamo.zig) --------------------------------------
 // per-radius density-weighted scale height, the reference's iy-outer / iz-inner
 // accumulation order kept (one thread per radial column)
-__global__ void k_scale_height(DevState s) {
-  long ix = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ix >= s.gr.nx) return;
-  long nc = s.gr.nc;
+// Per-radius scale height (dynamo.zig:158 calcScaleHeight). The fold over
+// (iy, iz) of each x column keeps the reference's serial order (iy outer, iz
+// inner), so it is one thread's job; a block serves 32 columns, its 8 warps
+// stage tiles of the fold's inputs in shared memory and lane ix of warp 0
+// folds them in order.
+constexpr int SH_COLS = 32, SH_WARPS = 8, SH_TILE = 48;
+__global__ void __launch_bounds__(256) k_scale_height(DevState s) {
+  __shared__ double t_rho[SH_TILE][SH_COLS], t_gd[SH_TILE][SH_COLS], t_th[SH_TILE][SH_COLS];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  long ix = (long)blockIdx.x * SH_COLS + lane;
+  bool okx = ix < s.gr.nx;
+  long nz = s.gr.nz, nsteps = (long)s.gr.ny * nz, nc = s.gr.nc;
   double sigma = 0.0, sth = 0.0;
-  for (long iy = 0; iy < s.gr.ny; ++iy)
-    for (long iz = 0; iz < s.gr.nz; ++iz) {
-      long c = cidx(s.gr, ix, iy, iz);
-      double gd = s.cgc[10L * nc + c];
-      double th = s.blg[27L * nc + c];
-      double rho = s.p[RHO * nc + c];
-      double dth = KP_PI / 2.0 - th;
-      sigma += rho * gd;
-      sth += rho * gd * dth * dth;
+  for (long k0 = 0; k0 < nsteps; k0 += SH_TILE) {
+    for (int j = warp; j < SH_TILE; j += SH_WARPS) {
+      long k = k0 + j;
+      if (k < nsteps && okx) {
+        long c = cidx(s.gr, ix, k / nz, k % nz);
+        t_rho[j][lane] = s.p[RHO * nc + c];
+        t_gd[j][lane] = s.cgc[10L * nc + c];
+        t_th[j][lane] = s.blg[27L * nc + c];
+      }
     }
-  s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
+    __syncthreads();
+    if (warp == 0 && okx) {
+      long m = nsteps - k0 < SH_TILE ? nsteps - k0 : SH_TILE;
+      for (int j = 0; j < m; ++j) {
+        double rho = t_rho[j][lane], gd = t_gd[j][lane];
+        double dth = KP_PI / 2.0 - t_th[j][lane];
+        sigma += rho * gd;
+        sth += rho * gd * dth * dth;
+      }
+    }
+    __syncthreads();
+  }
+  if (warp == 0 && okx) s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
 }
 struct DynArgs {
   double gam, dt, a, rhor, risco;

@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libkoralcuda.so")
+# KORALCUDA_LIB selects another build of the library (e.g. a debug build)
+LIB_PATH = os.environ.get("KORALCUDA_LIB") or os.path.join(HERE, "libkoralcuda.so")
 NV = 13
 NFLAGS = 6
 

@@ -38,7 +38,8 @@ enum {
   KC_ERR_NAN_IN_FLUX = 5,
   KC_ERR_CUDA = 6,
   KC_ERR_TIMEOUT = 7,
-  KC_ERR_NO_DEVICE = 8
+  KC_ERR_NO_DEVICE = 8,
+  KC_ERR_TOO_MANY_CELLS = 9 /* more cells than kc_implicit_batch_noalloc stages */
 };
 
 enum { KC_BC_PERIODIC = 0, KC_BC_COPY = 1, KC_BC_PUFFY = 2 };
@@ -209,6 +210,18 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
  * {ok, rung, iters, whichprim, whicheq, whichframe} per cell. */
 int kc_implicit_batch(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
                       int32_t* res, int32_t mode);
+/* kc_implicit_batch without any allocation (no counterpart in the reference):
+ * for callers that cannot allocate device memory, such as a host application
+ * whose device memory is owned by another allocator (a framework's caching
+ * allocator holding the device) or a fixed-budget process. The arrays are
+ * staged through one fixed device array of KC_NOALLOC_MAX_CELLS cells (5 MiB),
+ * held by every device that loads the library until exit; n above the maximum
+ * returns KC_ERR_TOO_MANY_CELLS. The first call on a device looks up that
+ * array's address with the device current (make that first call before any
+ * stream capture). Calls share the array: calls that overlap on one device race. */
+#define KC_NOALLOC_MAX_CELLS 16384
+int kc_implicit_batch_noalloc(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
+                              int32_t* res, int32_t mode);
 /* u2p cascade of one cell as calcU2p applies it (koral/sim.zig:972-994):
  * u2pMhd + u2pRad + both floors. flags_out: {entropy_used, hd_fixup, rad_fixup} */
 int kc_u2p_batch(const kc_options* opt, int64_t n, const double* geom23, const double* uu, double* pp,

@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1105,5 +1106,79 @@ extern "C" int kc_u2p_batch(const kc_options* opt, int64_t n, const double* geom
   if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
   cudaMemcpy(pp, dp.p, n * NV * 8, cudaMemcpyDeviceToHost);
   cudaMemcpy(flags_out, df.p, n * 3 * 4, cudaMemcpyDeviceToHost);
+  return KC_OK;
+}
+
+// ==== allocation-free implicit batch ==========================================
+// kc_implicit_batch stages the caller's host arrays through device buffers it
+// allocates per call. This variant stages them through one fixed, file-scope
+// device array instead and allocates nothing: 16384 cells of geometry (23 f64),
+// dt (1 f64), primitives (13 f64) and results (6 i32), 5 MiB, held by every
+// device that loads the library until the process exits. The address of the
+// array on a device is looked up once, with that device current, on the first
+// call on that device (that first call should come before any stream capture).
+// All calls on a device share the array and leave the last call's contents in
+// it; calls that overlap on the same device race on it.
+namespace {
+
+const size_t kNoAllocGeomOff = 0;
+const size_t kNoAllocDtOff = kNoAllocGeomOff + (size_t)KC_NOALLOC_MAX_CELLS * 23 * 8;
+const size_t kNoAllocPpOff = kNoAllocDtOff + (size_t)KC_NOALLOC_MAX_CELLS * 8;
+const size_t kNoAllocResOff = kNoAllocPpOff + (size_t)KC_NOALLOC_MAX_CELLS * NV * 8;
+const size_t kNoAllocBytes = kNoAllocResOff + (size_t)KC_NOALLOC_MAX_CELLS * 6 * 4;
+static_assert(kNoAllocDtOff % 256 == 0 && kNoAllocPpOff % 256 == 0 && kNoAllocResOff % 256 == 0,
+              "scratch regions stay 256-byte aligned");
+
+// host-side stand-in for the device array; its device address comes from
+// cudaGetSymbolAddress
+static __device__ __align__(256) unsigned char kc_noalloc_scratch[kNoAllocBytes];
+
+const int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// the scratch array's address on the current device (set-up on first use)
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return KC_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, kc_noalloc_scratch) != cudaSuccess || !ptr) return KC_ERR_CUDA;
+    g_noalloc_ptr[dev] = (unsigned char*)ptr;
+  }
+  *out = g_noalloc_ptr[dev];
+  return KC_OK;
+}
+
+}  // namespace
+
+extern "C" int kc_implicit_batch_noalloc(const kc_options* opt, int64_t n, const double* geom23, const double* dt,
+                                         double* pp, int32_t* res, int32_t mode) {
+  if (n > KC_NOALLOC_MAX_CELLS) return KC_ERR_TOO_MANY_CELLS;
+  BatchArgs a;
+  int st = batch_prepare(opt, a);
+  if (st) return st;
+  if (mode != KC_IMPLICIT_PER_CELL) return KC_ERR_INVALID_CONFIG;
+  if (n <= 0) return KC_OK;
+  if (!geom23 || !dt || !pp || !res) return KC_ERR_INVALID_CONFIG;
+  unsigned char* base = nullptr;
+  if ((st = noalloc_scratch(&base))) return st;
+  double* dg = (double*)(base + kNoAllocGeomOff);
+  double* dd = (double*)(base + kNoAllocDtOff);
+  double* dp = (double*)(base + kNoAllocPpOff);
+  int* dr = (int*)(base + kNoAllocResOff);
+  // every result entry of the n cells is written by the kernel; cleared anyway so
+  // that nothing of an earlier call can be read back
+  if (cudaMemset(dr, 0, (size_t)n * 6 * 4) != cudaSuccess ||
+      cudaMemcpy(dg, geom23, (size_t)n * 23 * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(dd, dt, (size_t)n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(dp, pp, (size_t)n * NV * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return KC_ERR_CUDA;
+  k_implicit_batch<<<nblk(n), TPB>>>(n, dg, dd, dp, dr, a);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  if (cudaMemcpy(pp, dp, (size_t)n * NV * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(res, dr, (size_t)n * 6 * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return KC_ERR_CUDA;
   return KC_OK;
 }

@@ -24,6 +24,8 @@ KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
 KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING = 0, 1
 KC_NPASS = 14
+KC_ERR_TOO_MANY_CELLS = 9
+KC_NOALLOC_MAX_CELLS = 16384
 
 
 class KcGrid(ctypes.Structure):
@@ -108,6 +110,7 @@ def lib():
     L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64, P(dbl)]
     L.kc_implicit_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
     L.kc_u2p_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp]
+    L.kc_implicit_batch_noalloc.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
     L.kc_set_pass_timing.argtypes = [vp, i32]
     L.kc_get_pass_times.argtypes = [vp, vp, vp]
     L.kc_pass_name.argtypes = [i32]
@@ -121,7 +124,7 @@ def lib():
               "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p", "kc_cfl_dt", "kc_step", "kc_step_n",
               "kc_set_precision", "kc_set_implicit_mode", "kc_set_guess", "kc_init_puffy", "kc_implicit_batch",
               "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
-              "kc_get_stream", "kc_get_launch_count"]:
+              "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -294,6 +297,21 @@ def implicit_batch(opt, geom23, dt, pp, mode=KC_IMPLICIT_PER_CELL):
                                  res.ctypes.data, mode)
     if st != KC_OK:
         raise KoralError(st, "kc_implicit_batch")
+    return pp, res
+
+
+def implicit_batch_noalloc(opt, geom23, dt, pp, mode=KC_IMPLICIT_PER_CELL):
+    """implicit_batch staged through the library's fixed device array (no
+    allocation); at most KC_NOALLOC_MAX_CELLS cells per call."""
+    geom23 = np.ascontiguousarray(geom23, dtype=np.float64)
+    dt = np.ascontiguousarray(dt, dtype=np.float64)
+    pp = np.array(pp, dtype=np.float64, order="C", copy=True)
+    n = pp.shape[0]
+    res = np.zeros((n, 6), dtype=np.int32)
+    st = lib().kc_implicit_batch_noalloc(ctypes.byref(opt), n, geom23.ctypes.data, dt.ctypes.data, pp.ctypes.data,
+                                         res.ctypes.data, mode)
+    if st != KC_OK:
+        raise KoralError(st, "kc_implicit_batch_noalloc")
     return pp, res
 
 

@@ -179,10 +179,124 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+IMPLICIT_MODES = {"per-cell": 0, "compacting": 1}
+IMPL_METRIC = "implicit M1 solves/s (batched, independent cells)"
+IMPL_UNIT = "solves/s"
+
+
+def oracle_implicit_rate(geom, dt, pp, threads, min_seconds=10.0):
+    """solves/s of the oracle's solveImplicitLab loop on host threads over the
+    given cells, repeated until min_seconds of work (a bounded sample)."""
+    import ctypes
+
+    import numpy as np
+
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    lib.orc_implicit_batch_mt.argtypes = [ctypes.c_long] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+    n = len(dt)
+    done, t = 0, 0.0
+    while t < min_seconds:
+        p = np.array(pp, copy=True)
+        res = np.zeros((n, 3), dtype=np.int32)
+        t0 = time.perf_counter()
+        lib.orc_implicit_batch_mt(n, geom.ctypes.data, dt.ctypes.data, p.ctypes.data, res.ctypes.data, threads)
+        t += time.perf_counter() - t0
+        done += n
+    return done / t, done, t
+
+
+def run_implicit(args, rank, world, local):
+    """The batched implicit M1 solve over 2^22 independent seeded cells
+    (kc_synth_implicit_cells), inputs resident in HBM, FP64."""
+    import numpy as np
+
+    kc = load_engine()
+    opt = kc.puffy_options(device=local)
+    n = args.cells
+    geom, dt, pp = kc.synth_implicit_cells(opt, n, args.seed + rank)
+    threads = os.cpu_count() or 1
+    sample_n = min(n, 1 << 14)
+    workload = f"{n} independent cells, seeded MKS2 states (kc_synth_implicit_cells), plain FP64"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rate, done, t = oracle_implicit_rate(geom[:sample_n], dt[:sample_n], pp[:sample_n], threads)
+        line = {"impl": "reference", "metric": IMPL_METRIC, "value": rate, "unit": IMPL_UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": workload},
+                "cpu_baseline": {"value": rate, "unit": IMPL_UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"first {sample_n} cells, {done} solves in {t:.1f} s"},
+                "e2e": {"value": rate, "unit": IMPL_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dg = torch.from_numpy(geom).cuda()
+    dd = torch.from_numpy(dt).cuda()
+    dp0 = torch.from_numpy(pp).cuda()
+    dp = torch.empty_like(dp0)
+    dr = torch.zeros((n, 6), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        dp.copy_(dp0)
+        kc.implicit_batch_device(opt, n, dg.data_ptr(), dd.data_ptr(), dp.data_ptr(), dr.data_ptr(), stream.cuda_stream,
+                                 mode=IMPLICIT_MODES[args.implicit_mode])
+
+    for _ in range(args.warmup):
+        launch()
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    res = dr.cpu().numpy()
+    ok = res[:, 0] == 1
+    value = n * args.steps / (ms / 1e3)
+    # end to end: host arrays through kc_implicit_batch (copies in and out inside)
+    ke = max(1, min(3, args.steps))
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        kc.implicit_batch(opt, geom, dt, pp, mode=IMPLICIT_MODES[args.implicit_mode])
+    te = time.perf_counter() - t0
+    bpc = (23 + 1 + 13 + 13) * B + 6 * 4
+    peaks, peak_kind = measured_peaks()
+    achieved = bpc * n / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": IMPL_METRIC, "value": value, "unit": IMPL_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cells)",
+        "config": {"workload": workload, "cells": n, "l2": "inputs larger than L2 (no flush)",
+                   "implicit_mode": args.implicit_mode,
+                   "converged": float(ok.mean()), "mean_iters": float(res[ok, 2].mean()),
+                   "rungs": np.bincount(res[ok, 1], minlength=6).tolist()},
+        "e2e": {"value": n * ke / te, "unit": IMPL_UNIT, "h2d_bytes_per_step": n * (23 + 1 + 13) * 8,
+                "d2h_bytes_per_step": n * (13 * 8 + 24), "steps": ke, "timer": "host wall clock (synchronous API)"},
+        "roofline": {"bound": "hbm", "kernel": "k_implicit_batch", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "algorithmic_bytes": bpc * n},
+        "clocks": clk, "gpu_launches": args.steps,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, done, t = oracle_implicit_rate(geom[:sample_n], dt[:sample_n], pp[:sample_n], threads)
+        line["cpu_baseline"] = {"value": rate, "unit": IMPL_UNIT, "cores": threads, "kind": "port",
+                                "sample": f"first {sample_n} cells, {done} solves in {t:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 20; 3 for --workload implicit)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="koral", choices=["koral", "reference"])
     ap.add_argument("--nx", type=int, default=192)
@@ -191,10 +305,19 @@ def main():
     ap.add_argument("--seed", type=int, default=20250)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="step", choices=["step", "implicit"],
+                    help="step: the RK2IMEX step on the wedge; implicit: the batched implicit-solve microbenchmark")
+    ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
+    ap.add_argument("--implicit-mode", default="compacting", choices=["per-cell", "compacting"],
+                    help="implicit solve form: one thread per cell, or the persistent lane-refilling state machine")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 3 if args.workload == "implicit" else 20
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.workload == "implicit":
+        return run_implicit(args, rank, world, local)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -217,7 +340,7 @@ def main():
 
     kc = load_engine()
     grid = kc.puffy_grid(args.nx, args.ny, args.nz)
-    opt = kc.puffy_options(device=local)
+    opt = kc.puffy_options(device=local, implicit_mode=IMPLICIT_MODES[args.implicit_mode])
     sim = kc.Sim(grid, opt)
     ncell = args.nx * args.ny * args.nz
     ndim = sum(1 for d in (args.nx, args.ny, args.nz) if d > 1)
@@ -321,7 +444,8 @@ def main():
         "dtype": "f64", "data": "synthetic (PUFFY torus from the engine's init + seeded 1e-3 rho/u_int noise)",
         "config": {"workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz} MKS2 (periodic phi), plain FP64",
                    "cells": ncell, "ghosts": 3, "precision": "plain FP64", "l2": "inputs larger than L2 (no flush)",
-                   "init_seconds": init_s, "beta_norm_factor": fac, "parallelism": f"replicas x{world}"},
+                   "init_seconds": init_s, "beta_norm_factor": fac, "parallelism": f"replicas x{world}",
+                   "implicit_mode": args.implicit_mode},
         "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": launches,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -210,6 +210,20 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
  * {ok, rung, iters, whichprim, whicheq, whichframe} per cell. */
 int kc_implicit_batch(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
                       int32_t* res, int32_t mode);
+/* kc_implicit_batch on device arrays: geom23, dt, pp and res are device
+ * pointers, the launch goes to `stream` (a cudaStream_t, NULL = default) and
+ * the call returns without waiting (no counterpart in the reference: the
+ * GPU-resident form of the same batch). */
+int kc_implicit_batch_device(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
+                             int32_t* res, int32_t mode, void* stream);
+/* Seeded synthetic cells for the batched implicit-solve microbenchmark (no
+ * reference counterpart; the distribution widens the reference's battery,
+ * tools/bench_implicit.zig): MKS2 geometry at r log-uniform in [3, 50] and
+ * theta uniform in [0.3, pi-0.3]; rho log-uniform in [1e-8, 1]; T_gas
+ * log-uniform in [1e5, 1e9] K; |v| < 0.9c in a random direction; B with beta
+ * log-uniform in [1, 1e3]; E_gas/E_rad log-uniform in [1e-4, 1e4]; radiation
+ * frame Lorentz factor in [1, 2]; dt log-uniform in [1e-10, 1]. Host arrays. */
+int kc_synth_implicit_cells(const kc_options* opt, int64_t n, uint64_t seed, double* geom23, double* dt, double* pp);
 /* kc_implicit_batch without any allocation (no counterpart in the reference):
  * for callers that cannot allocate device memory, such as a host application
  * whose device memory is owned by another allocator (a framework's caching

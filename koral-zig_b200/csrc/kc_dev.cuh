@@ -60,6 +60,7 @@ struct DevScalars {
   unsigned long long tsd_max_bits;  // ordered bits of the positive CFL maximum (0 = none)
   unsigned long long tsd_min_bits;
   unsigned long long n_fail, n_iters, n_solves, n_guard;
+  unsigned long long work_next;  // next work item of a persistent kernel
   int any_hd;      // some cell requested an hd fixup in the last u2p pass
   int err;         // first error code
   long long err_cell;

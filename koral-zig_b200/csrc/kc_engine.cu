@@ -57,6 +57,7 @@ struct kc_handle {
   // step scalars (koral/sim.zig:237-293)
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
+  int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
   // per-pass device time (koral/sim/timers.zig PassTimers), off by default:
   // an event is recorded at every pass boundary, and the interval up to the
   // next event belongs to the innermost pass open at the first (self time)
@@ -343,6 +344,22 @@ void launch_implicit(kc_handle* h, double dtin) {
   a.ip = h->sp.ip;
   a.polar_nc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
   PassScope ps(h, KC_PASS_IMPLICIT);
+  if (h->opt.implicit_mode == KC_IMPLICIT_COMPACTING) {
+    long nwork = (long)gr.nx * (gr.ny - 2L * a.polar_nc) * gr.nz;
+    if (h->impl_blocks == 0) {
+      int dev = 0, nsm = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_implicit_persistent, TPB, 0);
+      h->impl_blocks = (per_sm > 0 ? per_sm : 1) * (nsm > 0 ? nsm : 1);
+    }
+    long need = (nwork + TPB - 1) / TPB;
+    int blocks = (int)(need < h->impl_blocks ? need : h->impl_blocks);
+    cudaMemsetAsync(&h->dsc->work_next, 0, sizeof(unsigned long long), h->stream);
+    ++h->n_launch;
+    if (blocks > 0) k_implicit_persistent<<<blocks, TPB, 0, h->stream>>>(h->ds, h->dsc, a, nwork);
+    return;
+  }
   ++h->n_launch;
   k_implicit<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
 }
@@ -875,7 +892,8 @@ int kc_set_precision(kc_handle* h, int32_t mode) {
 }
 int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (mode != KC_IMPLICIT_PER_CELL) return fail(h, KC_ERR_INVALID_CONFIG, "implicit mode not built");
+  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING)
+    return fail(h, KC_ERR_INVALID_CONFIG, "unknown implicit mode");
   h->opt.implicit_mode = mode;
   return KC_OK;
 }
@@ -1045,6 +1063,71 @@ __global__ void __launch_bounds__(128) k_u2p_batch(long n, const double* __restr
   fl_out[i * 3 + 2] = rr.corrected ? -1 : 0;
 }
 
+// the batch as a persistent, lane-refilling solve (kc_implicit_sm.cuh)
+struct ImpBatchSrc {
+  const double* geom23;
+  const double* dt;
+  double* pp_io;
+  int* res;
+  __device__ bool load(long i, ImpLane& L) {
+    geom_from_record23(geom23 + i * 23, L.g);
+    for (int k = 0; k < NV; ++k) L.pp00[k] = pp_io[i * NV + k];
+    L.dt = dt[i];
+    L.cell = i;
+    return true;
+  }
+  __device__ void store(const ImpLane& L) {
+    long i = L.cell;
+    int* o = res + i * 6;
+    if (L.ok) {
+      for (int k = 0; k < NV; ++k) pp_io[i * NV + k] = L.pp[k];
+      o[0] = 1;
+      o[1] = L.rung;
+      o[2] = L.iters;
+      o[3] = L.p;
+      o[4] = L.e;
+      o[5] = L.fr;
+    } else {
+      o[0] = 0;
+      o[1] = -1;
+      o[2] = 0;
+      o[3] = PRIM_RAD;
+      o[4] = EQ_ENERGY;
+      o[5] = FRAME_LAB;
+    }
+  }
+};
+__global__ void __launch_bounds__(128) k_implicit_batch_persistent(long n, const double* geom23, const double* dt,
+                                                                   double* pp_io, int* res, BatchArgs a,
+                                                                   unsigned long long* counter) {
+  ImpBatchSrc src{geom23, dt, pp_io, res};
+  ImpParams P{a.gam, a.rp, a.op, a.ip};
+  imp_persistent(src, n, counter, P);
+}
+// launch either form of the batch on `st`; the persistent form takes a
+// zeroed counter from the stream-ordered allocator
+int launch_batch(long n, const double* g, const double* d, double* p, int* r, const BatchArgs& a, int mode,
+                 cudaStream_t st) {
+  if (mode == KC_IMPLICIT_PER_CELL) {
+    k_implicit_batch<<<nblk(n), TPB, 0, st>>>(n, g, d, p, r, a);
+    return cudaGetLastError() == cudaSuccess ? KC_OK : KC_ERR_CUDA;
+  }
+  if (mode != KC_IMPLICIT_COMPACTING) return KC_ERR_INVALID_CONFIG;
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_implicit_batch_persistent, TPB, 0);
+  long need = (n + TPB - 1) / TPB, cap = (long)(per_sm > 0 ? per_sm : 1) * (nsm > 0 ? nsm : 1);
+  void* counter = nullptr;
+  if (cudaMallocAsync(&counter, sizeof(unsigned long long), st) != cudaSuccess) return KC_ERR_OOM;
+  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+  k_implicit_batch_persistent<<<(unsigned)(need < cap ? need : cap), TPB, 0, st>>>(n, g, d, p, r, a,
+                                                                                   (unsigned long long*)counter);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(counter, st);
+  return e == cudaSuccess ? KC_OK : KC_ERR_CUDA;
+}
+
 struct DevBuf {
   void* p = nullptr;
   ~DevBuf() {
@@ -1073,7 +1156,7 @@ extern "C" int kc_implicit_batch(const kc_options* opt, int64_t n, const double*
   BatchArgs a;
   int st = batch_prepare(opt, a);
   if (st) return st;
-  if (mode != KC_IMPLICIT_PER_CELL) return KC_ERR_INVALID_CONFIG;
+  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING) return KC_ERR_INVALID_CONFIG;
   if (n <= 0) return KC_OK;
   DevBuf dg, dd, dp, dr;
   if (cudaMalloc(&dg.p, n * 23 * 8) || cudaMalloc(&dd.p, n * 8) || cudaMalloc(&dp.p, n * NV * 8) ||
@@ -1082,10 +1165,101 @@ extern "C" int kc_implicit_batch(const kc_options* opt, int64_t n, const double*
   cudaMemcpy(dg.p, geom23, n * 23 * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(dd.p, dt, n * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(dp.p, pp, n * NV * 8, cudaMemcpyHostToDevice);
-  k_implicit_batch<<<nblk(n), TPB>>>(n, (const double*)dg.p, (const double*)dd.p, (double*)dp.p, (int*)dr.p, a);
-  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  if ((st = launch_batch(n, (const double*)dg.p, (const double*)dd.p, (double*)dp.p, (int*)dr.p, a, mode, 0)))
+    return st;
+  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
   cudaMemcpy(pp, dp.p, n * NV * 8, cudaMemcpyDeviceToHost);
   cudaMemcpy(res, dr.p, n * 6 * 4, cudaMemcpyDeviceToHost);
+  return KC_OK;
+}
+
+extern "C" int kc_implicit_batch_device(const kc_options* opt, int64_t n, const double* geom23, const double* dt,
+                                        double* pp, int32_t* res, int32_t mode, void* stream) {
+  BatchArgs a;
+  int st = batch_prepare(opt, a);
+  if (st) return st;
+  if (n <= 0) return KC_OK;
+  if (!geom23 || !dt || !pp || !res) return KC_ERR_INVALID_CONFIG;
+  return launch_batch(n, geom23, dt, pp, res, a, mode, (cudaStream_t)stream);
+}
+
+namespace {
+// xorshift64* (the generator family of the reference's implicit battery)
+struct XorShift {
+  uint64_t s;
+  double next() {
+    s ^= s >> 12;
+    s ^= s << 25;
+    s ^= s >> 27;
+    return (double)((s * 0x2545F4914F6CDD1DULL) >> 11) * 0x1.0p-53;
+  }
+  double pm() { return 2.0 * next() - 1.0; }
+  double loguni(double lo, double hi) { return kmath::exp(kmath::log(lo) + (kmath::log(hi) - kmath::log(lo)) * next()); }
+};
+// a spatial 3-velocity (VELR) of Lorentz factor gamma relative to the normal
+// observer, in a random direction
+void velr_with_gamma(XorShift& rng, const Geom& g, double gamma, double v[3]) {
+  double nn[3] = {rng.pm(), rng.pm(), rng.pm()};
+  double q = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) q += nn[i] * nn[j] * g.gg[i + 1][j + 1];
+  double sc = kmath::sqrt((gamma * gamma - 1.0) / q);
+  for (int i = 0; i < 3; ++i) v[i] = nn[i] * sc;
+}
+}  // namespace
+
+extern "C" int kc_synth_implicit_cells(const kc_options* opt, int64_t n, uint64_t seed, double* geom23, double* dt,
+                                       double* pp) {
+  if (!opt || opt->abi_version != KC_ABI_VERSION || n < 0 || !geom23 || !dt || !pp) return KC_ERR_INVALID_CONFIG;
+  SimParams sp;
+  params_from_options(*opt, sp);
+  const Consts& con = sp.op.c;
+  const long nchunk = 4096;
+  host_par(0, (n + nchunk - 1) / nchunk, [&](long k) {
+    XorShift rng{seed ^ (0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1))};
+    for (long c = k * nchunk; c < n && c < (k + 1) * nchunk; ++c) {
+      double r = rng.loguni(3.0, 50.0);
+      double th = 0.3 + (KP_PI - 0.6) * rng.next();
+      double x[4] = {0.0, kmath::log(r - sp.mp.mksr0), mks2_x2_from_theta(th, sp.mp.mksh0), 0.0};
+      Geom g;
+      geometry_at(MKS2, sp.mp, x, g);
+      double* gr = geom23 + c * 23;
+      int q = 0;
+      for (int i = 0; i < 4; ++i)
+        for (int j = i; j < 4; ++j) {
+          gr[q] = g.gg[i][j];
+          gr[10 + q] = g.GG[i][j];
+          ++q;
+        }
+      gr[20] = g.gdet;
+      gr[21] = g.alpha;
+      gr[22] = g.gttpert;
+      double* p = pp + c * NV;
+      double rho = rng.loguni(1.0e-8, 1.0);
+      double tgas = rng.loguni(1.0e5, 1.0e9);
+      double ugas = u_from_trho(con, tgas, rho, sp.gam);
+      double v[3];
+      velr_with_gamma(rng, g, 1.0 / kmath::sqrt(1.0 - 0.81 * rng.next()), v);  // |v| < 0.9c
+      p[RHO] = rho;
+      p[UU] = ugas;
+      p[VX] = v[0];
+      p[VY] = v[1];
+      p[VZ] = v[2];
+      p[ENTR] = s_from_u(rho, ugas, sp.gam);
+      double beta = rng.loguni(1.0, 1.0e3);
+      double bsq = 2.0 * (sp.gam - 1.0) * ugas / beta;
+      velr_with_gamma(rng, g, kmath::sqrt(1.0 + bsq), v);
+      p[B1] = v[0];
+      p[B2] = v[1];
+      p[B3] = v[2];
+      p[EE] = ugas / rng.loguni(1.0e-4, 1.0e4);  // E_gas / E_rad log-uniform in [1e-4, 1e4]
+      velr_with_gamma(rng, g, 1.0 + rng.next(), v);
+      p[FX] = v[0];
+      p[FY] = v[1];
+      p[FZ] = v[2];
+      dt[c] = rng.loguni(1.0e-10, 1.0);
+    }
+  });
   return KC_OK;
 }
 

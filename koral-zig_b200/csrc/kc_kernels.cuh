@@ -5,6 +5,7 @@
 // (--fmad=false) reproduces the CPU oracle bit for bit.
 #pragma once
 #include "kc_dev.cuh"
+#include "kc_implicit_sm.cuh"
 
 namespace kc {
 
@@ -850,6 +851,14 @@ __global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, Im
     s.flags[5 * nc + c] = -1;
     atomicAdd(&sc->n_fail, 1ULL);
   }
+}
+
+// the same operator as a persistent, lane-refilling state machine (bit-identical)
+__global__ void __launch_bounds__(128) k_implicit_persistent(DevState s, DevScalars* sc, ImplArgs a, long nwork) {
+  long nyb = s.gr.ny - 2L * a.polar_nc;
+  ImpStepSrc src{s, sc, a.dt, s.gr.nx, nyb, (long)a.polar_nc};
+  ImpParams P{a.gam, a.rp, a.op, a.ip};
+  imp_persistent(src, nwork, &sc->work_next, P);
 }
 
 // ---- radiative viscosity (koral/sim/rijvisc.zig:266) ---------------------------

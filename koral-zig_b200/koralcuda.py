@@ -111,6 +111,8 @@ def lib():
     L.kc_implicit_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
     L.kc_u2p_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp]
     L.kc_implicit_batch_noalloc.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
+    L.kc_implicit_batch_device.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32, vp]
+    L.kc_synth_implicit_cells.argtypes = [P(KcOptions), i64, ctypes.c_uint64, vp, vp, vp]
     L.kc_set_pass_timing.argtypes = [vp, i32]
     L.kc_get_pass_times.argtypes = [vp, vp, vp]
     L.kc_pass_name.argtypes = [i32]
@@ -124,7 +126,8 @@ def lib():
               "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p", "kc_cfl_dt", "kc_step", "kc_step_n",
               "kc_set_precision", "kc_set_implicit_mode", "kc_set_guess", "kc_init_puffy", "kc_implicit_batch",
               "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
-              "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc"]:
+              "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc", "kc_implicit_batch_device",
+              "kc_synth_implicit_cells"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -313,6 +316,24 @@ def implicit_batch_noalloc(opt, geom23, dt, pp, mode=KC_IMPLICIT_PER_CELL):
     if st != KC_OK:
         raise KoralError(st, "kc_implicit_batch_noalloc")
     return pp, res
+
+
+def synth_implicit_cells(opt, n, seed):
+    """Seeded synthetic (geom23, dt, pp) cells of the implicit microbenchmark."""
+    geom23 = np.empty((n, 23))
+    dt = np.empty(n)
+    pp = np.empty((n, NV))
+    st = lib().kc_synth_implicit_cells(ctypes.byref(opt), n, seed, geom23.ctypes.data, dt.ctypes.data, pp.ctypes.data)
+    if st != KC_OK:
+        raise KoralError(st, "kc_synth_implicit_cells")
+    return geom23, dt, pp
+
+
+def implicit_batch_device(opt, n, geom23_ptr, dt_ptr, pp_ptr, res_ptr, stream=0, mode=KC_IMPLICIT_PER_CELL):
+    """Launch the batch solve on device arrays (raw pointers) without waiting."""
+    st = lib().kc_implicit_batch_device(ctypes.byref(opt), n, geom23_ptr, dt_ptr, pp_ptr, res_ptr, mode, stream)
+    if st != KC_OK:
+        raise KoralError(st, "kc_implicit_batch_device")
 
 
 def u2p_batch(opt, geom23, uu, pp):

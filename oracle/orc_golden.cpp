@@ -302,3 +302,37 @@ extern "C" int orc_golden(const char* name, long nrec, const double* in, int nin
   }
   return 0;
 }
+
+// solveImplicitLab over n independent cells on `nthreads` host threads, cells
+// handed out in chunks from an atomic ticket (the scheme of the reference's
+// tools/bench_implicit.zig:53-94). geom23 as the golden records; pp in/out;
+// res per cell {ok, rung, iters}. The CPU baseline of the implicit microbench.
+#include <atomic>
+#include <thread>
+#include <vector>
+extern "C" int orc_implicit_batch_mt(long n, const double* geom23, const double* dt, double* pp, int* res,
+                                     int nthreads) {
+  const RadParams rp = rad_params_puffy();
+  const OpacParams op = opac_params_puffy(10.0);
+  const ImplicitParams ip = implicit_params_puffy();
+  std::atomic<long> next(0);
+  const long chunk = 64;
+  auto work = [&]() {
+    for (long c0 = next.fetch_add(chunk); c0 < n; c0 = next.fetch_add(chunk)) {
+      for (long c = c0; c < n && c < c0 + chunk; ++c) {
+        Geom g;
+        geom_from_record(geom23 + c * 23, 23, g);
+        double uu[NV];
+        ImplicitResult r = solve_implicit_lab(uu, pp + c * NV, g, dt[c], kGam, rp, op, ip);
+        res[c * 3 + 0] = r.ok;
+        res[c * 3 + 1] = r.rung;
+        res[c * 3 + 2] = r.iters;
+      }
+    }
+  };
+  if (nthreads < 1) nthreads = 1;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t) th.emplace_back(work);
+  for (auto& t : th) t.join();
+  return 0;
+}

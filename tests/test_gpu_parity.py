@@ -19,11 +19,15 @@ def _kc():
     return kc
 
 
-def test_implicit_batch_bitwise_on_golden_records():
+MODES = [0, 1]  # KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING (persistent state machine)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_implicit_batch_bitwise_on_golden_records(mode):
     kc = _kc()
     i, _ = load_kgld("rad/rad_implicit")
     z = run_golden("rad_implicit", i, 19)
-    pp, res = kc.implicit_batch(kc.puffy_options(), i[:, :23], i[:, 23], i[:, 24:37])
+    pp, res = kc.implicit_batch(kc.puffy_options(), i[:, :23], i[:, 23], i[:, 24:37], mode=mode)
     ok = res[:, 0] == 1
     assert np.array_equal(ok, z[:, 0] == 0.0)
     assert np.array_equal(res[ok, 3], z[ok, 1].astype(int))  # whichprim
@@ -43,11 +47,11 @@ def test_u2p_batch_bitwise_on_golden_records():
     assert np.array_equal(fl, z[:, 13:16].astype(np.int32))
 
 
-def _start(name):
+def _start(name, mode=0):
     kc = _kc()
     z = np.load(f"{GOLDEN}/{name}_kslf.npz")
     nx, ny = int(z["nx"]), int(z["ny"])
-    grid, opt = kc.puffy_grid(nx, ny), kc.puffy_options()
+    grid, opt = kc.puffy_grid(nx, ny), kc.puffy_options(implicit_mode=mode)
     gpu = kc.Sim(grid, opt)
     orc = OracleSim(grid, opt)
     sc = z["scalars"][0]
@@ -71,9 +75,10 @@ def _diff_report(a, b):
     return f"{len(bad[0])} differing entries; first at {[x[:5] for x in bad]}"
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("nsteps", [1, 3])
-def test_step_bitwise_vs_oracle_puffy_fast(nsteps):
-    z, gpu, orc = _start("puffy_fast")
+def test_step_bitwise_vs_oracle_puffy_fast(nsteps, mode):
+    z, gpu, orc = _start("puffy_fast", mode)
     for _ in range(nsteps):
         gpu.step()
         orc.step()
@@ -91,7 +96,8 @@ def test_step_bitwise_vs_oracle_puffy_fast(nsteps):
 
 def _pair(grid, opt):
     kc = _kc()
-    return kc.Sim(grid, opt), OracleSim(grid, opt)
+    orc_opt = kc.puffy_options()
+    return kc.Sim(grid, opt), OracleSim(grid, orc_opt)
 
 
 def _assert_same_state(gpu, orc):
@@ -114,11 +120,12 @@ def test_init_bitwise_vs_oracle_puffy_fast():
     _assert_same_state(gpu, orc)
 
 
-def test_init_perturbed_3d_then_steps_bitwise():
+@pytest.mark.parametrize("mode", MODES)
+def test_init_perturbed_3d_then_steps_bitwise(mode):
     """The bench's workload shape in small: a 3D wedge with periodic phi, the
     seeded 1e-3 u_int / rho perturbations, then CFL steps."""
     kc = _kc()
-    grid, opt = kc.puffy_grid(24, 20, 8), kc.puffy_options()
+    grid, opt = kc.puffy_grid(24, 20, 8), kc.puffy_options(implicit_mode=mode)
     gpu, orc = _pair(grid, opt)
     fg = gpu.initPuffy(1e-3, 1e-3, 12345)
     fo = orc.init_puffy(1e-3, 1e-3, 12345)
@@ -134,15 +141,16 @@ def test_init_perturbed_3d_then_steps_bitwise():
     _assert_same_state(gpu, orc)
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", ["puffy64", "puffy3d"])
-def test_forced_dt_steps_bitwise_from_c_state(name):
+def test_forced_dt_steps_bitwise_from_c_state(name, mode):
     """C KORAL's post-init state of the forced-dt step goldens (64x60, and the
     32x30x4 wedge), stepped with C's dt sequence on both sides."""
     from tests.test_oracle_kstp import load_domain
 
     kc = _kc()
     z = np.load(f"{GOLDEN}/{name}_kstp.npz")
-    grid, opt = kc.puffy_grid(int(z["nx"]), int(z["ny"]), int(z["nz"])), kc.puffy_options()
+    grid, opt = kc.puffy_grid(int(z["nx"]), int(z["ny"]), int(z["nz"])), kc.puffy_options(implicit_mode=mode)
     gpu, orc = _pair(grid, opt)
     load_domain(orc, grid, z, 0)
     gpu.set_prims(orc.prims())

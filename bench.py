@@ -308,7 +308,7 @@ def main():
     ap.add_argument("--workload", default="step", choices=["step", "implicit"],
                     help="step: the RK2IMEX step on the wedge; implicit: the batched implicit-solve microbenchmark")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
-    ap.add_argument("--implicit-mode", default="compacting", choices=["per-cell", "compacting"],
+    ap.add_argument("--implicit-mode", default="per-cell", choices=["per-cell", "compacting"],
                     help="implicit solve form: one thread per cell, or the persistent lane-refilling state machine")
     args = ap.parse_args()
     if args.steps is None:

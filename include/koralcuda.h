@@ -157,6 +157,19 @@ int kc_download_flags(kc_handle* h, int32_t* flags);
 int kc_set_counters(kc_handle* h, const kc_counters* c);
 int kc_get_counters(kc_handle* h, kc_counters* c);
 
+/* One row of the diagnostics time series (koral/io/dump.zig:414 ScalarRow),
+ * code units: mass (scalars.zig:78 totalMass), mdot through the horizon shell
+ * (>0 for accretion, scalars.zig:106), radiative and total luminosity through
+ * the shell at r_lum in BL (scalars.zig:136, type 1), density-weighted scale
+ * height at r_scale (dynamo.zig:239), max pmag/ptot (scalars.zig:276), and the
+ * counts of dump.zig:358 collectDiag plus the solver counters. */
+typedef struct kc_scalar_row {
+  double t, dt;
+  int64_t nstep;
+  double mass, mdot, radlum, totallum, scaleheight, max_pmag_ptot;
+  int64_t n_hd_fixup, n_radimp_fail, n_nan, n_floorguard;
+} kc_scalar_row;
+
 /* PUFFY initial state: puffy.initAllWith (koral/problems/puffy/puffy.zig:873)
  * — limotorus, atmosphere, A_phi seed, set_bc, B from A, set_bc, beta
  * normalization — followed by Sim.initTimestepGuess, as
@@ -168,6 +181,11 @@ int kc_get_counters(kc_handle* h, kc_counters* c);
  * seed ^ 0x5DEECE66D). fac_out (may be NULL) receives the normalization
  * factor sqrt(maxbeta / max beta) that initAllWith returns. */
 int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t seed, double* fac_out);
+/* dump.scalarRow (koral/io/dump.zig:383) on the current state; `dt` is only
+ * recorded. PUFFY's driver uses r_lum = 5000, r_scale = 15
+ * (koral/problems/puffy/main.zig:30). The sums are folded in the reference's
+ * serial cell order, so the row is bit-identical to a serial evaluation. */
+int kc_scalars(kc_handle* h, double dt, double r_lum, double r_scale, kc_scalar_row* out);
 /* Sim.finishInit (koral/sim.zig:686): ghost fill from p, then the dt guess */
 int kc_finish_init(kc_handle* h);
 /* Sim.initTimestepGuess (koral/sim.zig:693) */

@@ -28,6 +28,15 @@ KC_ERR_TOO_MANY_CELLS = 9
 KC_NOALLOC_MAX_CELLS = 16384
 
 
+class KcScalarRow(ctypes.Structure):
+    """kc_scalar_row: one row of the diagnostics series (koral/io/dump.zig:414)."""
+    _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("nstep", ctypes.c_int64),
+                ("mass", ctypes.c_double), ("mdot", ctypes.c_double), ("radlum", ctypes.c_double),
+                ("totallum", ctypes.c_double), ("scaleheight", ctypes.c_double), ("max_pmag_ptot", ctypes.c_double),
+                ("n_hd_fixup", ctypes.c_int64), ("n_radimp_fail", ctypes.c_int64), ("n_nan", ctypes.c_int64),
+                ("n_floorguard", ctypes.c_int64)]
+
+
 class KcGrid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("ng", ctypes.c_int32),
                 ("minx", ctypes.c_double), ("maxx", ctypes.c_double), ("miny", ctypes.c_double),

@@ -1404,7 +1404,8 @@ int step(OSim& s, double forced_dt) {
 // postinit (puffy.zig:892: global beta max over the domain, B scaled by
 // sqrt(maxbeta/maxb), ghosts keep their unscaled B). Returns the error code;
 // `fac` receives the beta normalization factor.
-int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, double& fac) {
+// stage 0: prepinit + p2u over the domain, then set_bc (A_phi in the B slots)
+int init_stage0(OSim& s, double perturb, double perturb_rho, uint64_t seed) {
   const Grid& g = s.g;
   kcinit::PuffyPhysics ph;
   ph.mass = s.opt.mass;
@@ -1437,8 +1438,11 @@ int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, doubl
   });
   for (int e : errs)
     if (e) return e;
-  int e = set_bc(s);
-  if (e) return e;
+  return set_bc(s);
+}
+// stage 1: calc_BfromA with overwrite (ghosts take the zero scratch), set_bc
+int init_stage1(OSim& s) {
+  const Grid& g = s.g;
   std::fill(s.vecpot.begin(), s.vecpot.end(), 0.0);
   curl_from_a(s, s.p, NV, B1);
   for (long iz = -g.ngz; iz < g.nz + g.ngz; ++iz)
@@ -1453,7 +1457,12 @@ int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, doubl
         s.geom(ix, iy, iz, geo);
         p2u(pp, s.U(ix, iy, iz), geo, s.sp.gam);
       }
-  if ((e = set_bc(s))) return e;
+  return set_bc(s);
+}
+// stage 2: postinit beta normalization of the domain B (ghosts keep theirs)
+void init_stage2(OSim& s, double& fac) {
+  const Grid& g = s.g;
+  kcinit::PuffyPhysics ph;
   double maxb = 0.0;
   for (long iz = 0; iz < g.nz; ++iz)
     for (long iy = 0; iy < g.ny; ++iy)
@@ -1482,7 +1491,160 @@ int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, doubl
         s.geom(ix, iy, iz, geo);
         p2u(pp, s.U(ix, iy, iz), geo, s.sp.gam);
       }
+}
+
+// ---- diagnostics (koral/io/scalars.zig, koral/io/dump.zig:358-410) -----------
+// r_BL of a radial index (scalars.zig:47 radiusBL)
+double radius_bl(const OSim& s, long ix) {
+  double xx[4] = {0.0, grid_xc(s.g, ix), grid_yc(s.g, 0), grid_zc(s.g, 0)}, o[4];
+  mks2_to_bl(xx, s.sp.mp, o);
+  return o[1];
+}
+// scalars.zig:58 radialShellIndex
+long radial_shell_index(const OSim& s, double radius) {
+  for (long ix = 0; ix < s.g.nx; ++ix)
+    if (radius_bl(s, ix) > radius) return ix;
+  return s.g.nx - 1;
+}
+// BL theta / phi widths of a cell (scalars.zig:190,199)
+double bl_theta_width(const OSim& s, long ix, long iy, long iz) {
+  double a[4] = {0.0, grid_xc(s.g, ix), grid_yl(s.g, iy), grid_zc(s.g, iz)}, oa[4];
+  double b[4] = {0.0, grid_xc(s.g, ix), grid_yl(s.g, iy + 1), grid_zc(s.g, iz)}, ob[4];
+  mks2_to_bl(a, s.sp.mp, oa);
+  mks2_to_bl(b, s.sp.mp, ob);
+  return kmath::fabs(ob[2] - oa[2]);
+}
+double bl_phi_width(const OSim& s, long ix, long iy, long iz) {
+  double a[4] = {0.0, grid_xc(s.g, ix), grid_yc(s.g, iy), grid_zl(s.g, iz)}, oa[4];
+  double b[4] = {0.0, grid_xc(s.g, ix), grid_yc(s.g, iy), grid_zl(s.g, iz + 1)}, ob[4];
+  mks2_to_bl(a, s.sp.mp, oa);
+  mks2_to_bl(b, s.sp.mp, ob);
+  return kmath::fabs(ob[3] - oa[3]);
+}
+// dump.zig:383 scalarRow with scalars.zig:225 globalScalars (serial order)
+int scalar_row(OSim& s, double dt, double r_lum, double r_scale, kc_scalar_row& row) {
+  const Grid& g = s.g;
+  const double pi = KP_PI;
+  const bool twod = g.nz == 1;
+  long ix_h = radial_shell_index(s, r_horizon_bl(s.sp.mp.a));
+  long ix_l = radial_shell_index(s, r_lum);
+  // collectDiag (dump.zig:358)
+  long n_nan = 0, n_hd = 0;
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy)
+      for (long ix = 0; ix < g.nx; ++ix) {
+        const double* pp = s.P(ix, iy, iz);
+        for (int iv = 0; iv < NV; ++iv)
+          if (!kmath::isfinite(pp[iv])) {
+            n_nan += 1;
+            break;
+          }
+        if (s.flag(F_HD, ix, iy, iz) != 0) n_hd += 1;
+      }
+  // totalMass (scalars.zig:78)
+  double phifac = g.nz > 1 ? 2.0 * pi / (g.maxz - g.minz) : 1.0;
+  double mass = 0.0;
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy)
+      for (long ix = 0; ix < g.nx; ++ix) {
+        double dx = cell_size(g, ix, 0), dy = cell_size(g, iy, 1), dz = cell_size(g, iz, 2) * phifac;
+        mass += s.P(ix, iy, iz)[RHO] * dx * dy * dz * s.cgdet(ix, iy, iz);
+      }
+  // mdot (scalars.zig:106)
+  double mdot = 0.0;
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy) {
+      const double* pp = s.P(ix_h, iy, iz);
+      Geom geo;
+      s.geom(ix_h, iy, iz, geo);
+      double vcon[4] = {0.0, pp[VX], pp[VY], pp[VZ]}, ucon[4];
+      int e = convert(vcon, VELR, VEL4, geo, RECOMPUTE_UT, ucon);
+      if (e) return e;
+      double rhouconr = pp[RHO] * ucon[1];
+      double dy = cell_size(g, iy, 1);
+      double dz = twod ? 2.0 * pi : cell_size(g, iz, 2) * (2.0 * pi / (g.maxz - g.minz));
+      mdot += geo.gdet * rhouconr * dy * dz;
+    }
+  // lum, type 1 (scalars.zig:136)
+  double radlum = 0.0, totallum = 0.0;
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy) {
+      double pp[NV];
+      for (int i = 0; i < NV; ++i) pp[i] = s.P(ix_l, iy, iz)[i];
+      Geom geo;
+      s.geom(ix_l, iy, iz, geo);
+      const Geom& gbl = s.blg[s.ci(ix_l, iy, iz)];
+      double jac[4][4];
+      s.jac_bl(ix_l, iy, iz, jac);
+      int e = trans_pmhd_coco_j(pp, geo, gbl, jac, pp);
+      if (!e) e = trans_prad_coco_j(pp, geo, gbl, jac, pp);
+      if (e) return e;
+      double dth = bl_theta_width(s, ix_l, iy, iz);
+      double dph = twod ? 2.0 * pi : bl_phi_width(s, ix_l, iy, iz) * (2.0 * pi / (g.maxz - g.minz));
+      double vcon[4] = {0.0, pp[VX], pp[VY], pp[VZ]}, ucon[4];
+      if ((e = convert(vcon, VELR, VEL4, gbl, RECOMPUTE_UT, ucon))) return e;
+      double rhour = pp[RHO] * ucon[1];
+      double tup[4][4], tij[4][4], rup[4][4], rij[4][4];
+      calc_tij(pp, gbl, s.sp.gam, tup);
+      lower_second(tup, gbl, tij);
+      double trt = tij[1][0];
+      calc_rij(pp, gbl, rup);
+      lower_second(rup, gbl, rij);
+      double rrt = -rij[1][0];
+      if (rrt < 0.0) rrt = 0.0;
+      radlum += gbl.gdet * rrt * dth * dph;
+      totallum += gbl.gdet * (rhour + trt + rrt) * dth * dph;
+    }
+  // scale height (dynamo.zig:239 parts, :267 finalize)
+  long ix_s = radial_shell_index(s, r_scale);
+  double sig = 0.0, sth = 0.0;
+  for (long iy = 0; iy < g.ny; ++iy)
+    for (long iz = 0; iz < g.nz; ++iz) {
+      double gd = s.cgdet(ix_s, iy, iz);
+      double th = s.blg[s.ci(ix_s, iy, iz)].xx[2];
+      double rho = s.P(ix_s, iy, iz)[RHO];
+      double dth = pi / 2.0 - th;
+      sig += rho * gd;
+      sth += rho * gd * dth * dth;
+    }
+  // maxPmagPtot (scalars.zig:276)
+  double maxb = 0.0;
+  for (long iz = 0; iz < g.nz; ++iz)
+    for (long iy = 0; iy < g.ny; ++iy)
+      for (long ix = 0; ix < g.nx; ++ix) {
+        const double* pp = s.P(ix, iy, iz);
+        Geom geo;
+        s.geom(ix, iy, iz, geo);
+        double ucon[4], ucov[4], bcon[4], bcov[4], bsq;
+        ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], geo, ucon, ucov);
+        double B[3] = {pp[B1], pp[B2], pp[B3]};
+        bcon_bcov_bsq(B, ucon, ucov, geo, bcon, bcov, bsq);
+        double pmag = bsq / 2.0;
+        double ptot = (s.sp.gam - 1.0) * pp[UU];
+        ptot += (-calc_ff_rtt(pp, geo, nullptr)) / 3.0;
+        if (pmag / ptot > maxb) maxb = pmag / ptot;
+      }
+  row.t = s.t;
+  row.dt = dt;
+  row.nstep = s.nstep;
+  row.mass = mass;
+  row.mdot = -mdot;
+  row.radlum = radlum;
+  row.totallum = totallum;
+  row.scaleheight = ix_s > 0 ? kmath::sqrt(sth / sig) : sth;
+  row.max_pmag_ptot = maxb;
+  row.n_hd_fixup = n_hd;
+  row.n_radimp_fail = s.n_radimp_failures;
+  row.n_nan = n_nan;
+  row.n_floorguard = s.n_guard;
   return E_OK;
+}
+
+int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, double& fac) {
+  int e = init_stage0(s, perturb, perturb_rho, seed);
+  if (!e) e = init_stage1(s);
+  if (!e) init_stage2(s, fac);
+  return e;
 }
 
 }  // namespace
@@ -1600,6 +1762,21 @@ int orc_sim_calc_u2p(void* h) { return calc_u2p(*(OSim*)h); }
 int orc_sim_step(void* h, double forced_dt) { return step(*(OSim*)h, forced_dt); }
 int orc_sim_init_puffy(void* h, double perturb, double perturb_rho, unsigned long long seed, double* fac) {
   return init_puffy(*(OSim*)h, perturb, perturb_rho, seed, *fac);
+}
+int orc_sim_scalar_row(void* h, double dt, double r_lum, double r_scale, kc_scalar_row* row) {
+  return scalar_row(*(OSim*)h, dt, r_lum, r_scale, *row);
+}
+// one stage of the init sequence on the current state (0: prepinit + set_bc,
+// 1: B from A + set_bc, 2: beta normalization), for the C init goldens
+int orc_sim_init_stage(void* h, int stage, double perturb, double perturb_rho, unsigned long long seed, double* fac) {
+  OSim& s = *(OSim*)h;
+  if (stage == 0) return init_stage0(s, perturb, perturb_rho, seed);
+  if (stage == 1) return init_stage1(s);
+  if (stage == 2) {
+    init_stage2(s, *fac);
+    return 0;
+  }
+  return -1;
 }
 // single passes, for localizing engine-vs-oracle differences
 int orc_sim_phase(void* h, int phase, double dt) {

@@ -8,6 +8,10 @@ The reference (koral-zig) keeps three golden families for the step path:
             gzipped: "KSTP" u32 version, u32 nx,ny,nz,nv, u64 nrec, then per
             record {t, dt, u[ncell*nv], p[ncell*nv], flags[nf*ncell]}
   * KSLF  — Zig self-goldens (koral/testing/selfgolden.zig:20), gzipped.
+  * KINI  — C KORAL's PUFFY t=0 init snapshots (golden.zig:313 readKini),
+            gzipped: "KINI" u32 version, i32 nx,ny,nz,gx,gy,gz,stride,nvars,
+            i32 vars[nvars], f64 data[] (iz slowest, then iy, ix, vars fastest;
+            ghosts included when gx/gy > 0, else a stride-sampled domain).
 
 This script is run once where the reference tree is available; its outputs
 under tests/golden/ are what the test suite (and the GPU box) reads.
@@ -30,7 +34,9 @@ KGLD = [
     "rad/rad_rij.kgld", "rad/rad_u2prad.kgld", "rad/rad_wavespeeds.kgld", "rad/rad_floors.kgld",
     "rad/rad_thermo.kgld", "rad/rad_opac.kgld", "rad/rad_gi.kgld", "rad/rad_implicit.kgld",
     "metric/metric_points.kgld", "metric/coco_dxdx.kgld", "metric/krzysie_grid.kgld",
+    "init/puffy_scalars.kgld",
 ]
+KINI = ["init/puffy_t0_A.kini.gz", "init/puffy_t0_eps12.kini.gz", "init/puffy_t0_pfinal.kini.gz"]
 KSLF = ["puffy_fast.kslf", "puffy_full.kslf"]
 KSTP = ["step/puffy64.kstp.gz", "step/puffy3d.kstp.gz"]
 
@@ -87,12 +93,26 @@ def conv_kstp(src, dst):
                         flags=vals[:, 2 + 2 * nu:].reshape(nrec, ncell, nf).astype(np.int32))
 
 
+def conv_kini(src, dst):
+    raw = read_maybe_gz(src)
+    assert raw[:4] == b"KINI" and struct.unpack("<I", raw[4:8])[0] == 1
+    nx, ny, nz, gx, gy, gz, stride, nvars = struct.unpack("<8i", raw[8:40])
+    vars_ = np.frombuffer(raw[40:40 + 4 * nvars], dtype="<i4").copy()
+    sx = nx + 2 * gx if gx > 0 else (nx + stride - 1) // stride
+    sy = ny + 2 * gy if gy > 0 else (ny + stride - 1) // stride
+    data = np.frombuffer(raw[40 + 4 * nvars:], dtype="<f8").reshape(nz, sy, sx, nvars)
+    np.savez_compressed(dst, nx=nx, ny=ny, nz=nz, gx=gx, gy=gy, gz=gz, stride=stride, vars=vars_, data=data)
+
+
 def main(ref):
     for rel in KGLD:
         dst = os.path.join(HERE, rel.replace("/", "__").replace(".kgld", ".npz"))
         conv_kgld(os.path.join(ref, "tests/golden", rel), dst)
     for rel in KSLF:
         conv_kslf(os.path.join(ref, "tests/selfgolden", rel), os.path.join(HERE, rel.replace(".kslf", "_kslf.npz")))
+    for rel in KINI:
+        name = os.path.basename(rel).replace(".kini.gz", "_kini.npz")
+        conv_kini(os.path.join(ref, "tests/golden", rel), os.path.join(HERE, name))
     for rel in KSTP:
         name = os.path.basename(rel).replace(".kstp.gz", "_kstp.npz")
         conv_kstp(os.path.join(ref, "tests/golden", rel), os.path.join(HERE, name))

@@ -15,7 +15,7 @@ NFL = 6
 from tests.engine import koralcuda
 
 _kc = koralcuda()
-KcGrid, KcOptions, KcCounters = _kc.KcGrid, _kc.KcOptions, _kc.KcCounters
+KcGrid, KcOptions, KcCounters, KcScalarRow = _kc.KcGrid, _kc.KcOptions, _kc.KcCounters, _kc.KcScalarRow
 
 
 _sim_bound = False
@@ -53,6 +53,12 @@ def _bind():
     lib.orc_sim_init_puffy.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong,
                                        ctypes.POINTER(ctypes.c_double)]
     lib.orc_sim_init_puffy.restype = ctypes.c_int
+    lib.orc_sim_init_stage.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong,
+                                       ctypes.POINTER(ctypes.c_double)]
+    lib.orc_sim_init_stage.restype = ctypes.c_int
+    lib.orc_sim_scalar_row.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.POINTER(KcScalarRow)]
+    lib.orc_sim_scalar_row.restype = ctypes.c_int
     lib.orc_options_puffy.argtypes = [ctypes.POINTER(KcOptions)]
     lib.orc_grid_puffy.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(KcGrid)]
     _sim_bound = True
@@ -140,6 +146,22 @@ class OracleSim:
         if rc:
             raise RuntimeError(f"oracle init failed with status {rc}")
         return fac.value
+
+    def init_stage(self, stage, perturb=0.0, perturb_rho=0.0, seed=0):
+        """One stage of the init: 0 prepinit + set_bc, 1 B from A + set_bc,
+        2 beta normalization (returns the factor)."""
+        fac = ctypes.c_double(0.0)
+        rc = self.lib.orc_sim_init_stage(self.h, stage, perturb, perturb_rho, seed, ctypes.byref(fac))
+        if rc:
+            raise RuntimeError(f"oracle init stage {stage} failed with status {rc}")
+        return fac.value
+
+    def scalar_row(self, dt=0.0, r_lum=5000.0, r_scale=15.0):
+        row = KcScalarRow()
+        rc = self.lib.orc_sim_scalar_row(self.h, dt, r_lum, r_scale, ctypes.byref(row))
+        if rc:
+            raise RuntimeError(f"oracle scalar row failed with status {rc}")
+        return {k: getattr(row, k) for k, _ in KcScalarRow._fields_}
 
     def phase(self, which, dt=0.0):
         return self.lib.orc_sim_phase(self.h, which, dt)

@@ -58,6 +58,12 @@ struct kc_handle {
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
   int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
+  // scalar diagnostics: fold outputs and counts, and the BL geometry of the
+  // luminosity shell (built on the host at first use for that shell)
+  double* diag = nullptr;
+  long lum_ix = -1;
+  Geom* lum_gbl = nullptr;
+  double* lum_w = nullptr;
   // per-pass device time (koral/sim/timers.zig PassTimers), off by default:
   // an event is recorded at every pass boundary, and the interval up to the
   // next event belongs to the innermost pass open at the first (self time)
@@ -662,6 +668,7 @@ int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
   h->staging = dalloc<double>(h, NV * nc, st);
   h->flag_staging = dalloc<int>(h, 6 * nc, st);
   h->dsc = dalloc<DevScalars>(h, 1, st);
+  h->diag = dalloc<double>(h, 16, st);
   if (st) return st;
   // set_grid min-size scan with C's mdx quirk (koral/sim.zig:443)
   double mdx = -1, mdy = -1, mdz = -1;
@@ -783,6 +790,113 @@ int kc_calc_u2p(kc_handle* h) {
   int st = sync_check(h, "calc_u2p");
   return st ? st : collect_step_scalars(h, false);
 }
+// dump.scalarRow (koral/io/dump.zig:383) with scalars.zig:225 globalScalars
+namespace {
+double radius_bl_at(const kc_handle* h, long ix) {
+  const Grid& g = h->gr.g;
+  double xx[4] = {0.0, grid_xc(g, ix), grid_yc(g, 0), grid_zc(g, 0)}, o[4];
+  mks2_to_bl(xx, h->sp.mp, o);
+  return o[1];
+}
+long shell_index(const kc_handle* h, double radius) {
+  for (long ix = 0; ix < h->gr.nx; ++ix)
+    if (radius_bl_at(h, ix) > radius) return ix;
+  return h->gr.nx - 1;
+}
+}  // namespace
+
+int kc_scalars(kc_handle* h, double dt, double r_lum, double r_scale, kc_scalar_row* out) {
+  if (!h || !out) return KC_ERR_INVALID_CONFIG;
+  const DGrid& gr = h->gr;
+  const Grid& g = gr.g;
+  const double pi = KP_PI;
+  const bool twod = gr.nz == 1;
+  long ix_h = shell_index(h, r_horizon_bl(h->sp.mp.a));
+  long ix_l = shell_index(h, r_lum);
+  long ix_s = shell_index(h, r_scale);
+  long nyz = (long)gr.ny * gr.nz, ndom = (long)gr.nx * nyz;
+  int st = KC_OK;
+  if (h->lum_ix != ix_l) {
+    // BL geometry and BL cell widths of the luminosity shell (scalars.zig:190,199)
+    std::vector<Geom> gb(nyz);
+    std::vector<double> w(2 * nyz);
+    host_par(0, nyz, [&](long t) {
+      long iy = t % gr.ny, iz = t / gr.ny;
+      geometry_bl_at(g, h->sp.mp, ix_l, iy, iz, gb[t]);
+      double a[4] = {0.0, grid_xc(g, ix_l), grid_yl(g, iy), grid_zc(g, iz)}, oa[4];
+      double b[4] = {0.0, grid_xc(g, ix_l), grid_yl(g, iy + 1), grid_zc(g, iz)}, ob[4];
+      mks2_to_bl(a, h->sp.mp, oa);
+      mks2_to_bl(b, h->sp.mp, ob);
+      w[t] = kmath::fabs(ob[2] - oa[2]);
+      double c[4] = {0.0, grid_xc(g, ix_l), grid_yc(g, iy), grid_zl(g, iz)}, oc[4];
+      double d[4] = {0.0, grid_xc(g, ix_l), grid_yc(g, iy), grid_zl(g, iz + 1)}, od[4];
+      mks2_to_bl(c, h->sp.mp, oc);
+      mks2_to_bl(d, h->sp.mp, od);
+      w[nyz + t] = twod ? 2.0 * pi : kmath::fabs(od[3] - oc[3]) * (2.0 * pi / (g.maxz - g.minz));
+    });
+    if (!h->lum_gbl) h->lum_gbl = dalloc<Geom>(h, nyz, st);
+    if (!h->lum_w) h->lum_w = dalloc<double>(h, 2 * nyz, st);
+    if (st) return st;
+    cudaMemcpy(h->lum_gbl, gb.data(), nyz * sizeof(Geom), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->lum_w, w.data(), 2 * nyz * sizeof(double), cudaMemcpyHostToDevice);
+    h->lum_ix = ix_l;
+  }
+  // term buffers in the AoS staging area (unused between uploads/downloads)
+  double* mass_t = h->staging;
+  double* mdot_t = mass_t + ndom;
+  double* rad_t = mdot_t + nyz;
+  double* tot_t = rad_t + nyz;
+  double* scaleth = tot_t + nyz;
+  double* res = h->diag;  // mass, mdot, radlum, totallum; [8..9] counts
+  reset_step_scalars(h);
+  cudaMemsetAsync(res, 0, 16 * sizeof(double), h->stream);
+  double phifac = gr.nz > 1 ? 2.0 * pi / (g.maxz - g.minz) : 1.0;
+  k_diag_cells<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, phifac, mass_t, (unsigned long long*)(res + 8));
+  double dzfac = twod ? 0.0 : 2.0 * pi / (g.maxz - g.minz);
+  k_diag_mdot<<<nblk(nyz), TPB, 0, h->stream>>>(h->ds, h->dsc, ix_h, dzfac, mdot_t);
+  k_diag_lum<<<nblk(nyz), TPB, 0, h->stream>>>(h->ds, h->dsc, ix_l, h->sp.gam, h->lum_gbl, h->lum_w,
+                                                 h->lum_w + nyz, rad_t, tot_t);
+  k_fold_ordered<<<1, 256, 0, h->stream>>>(mass_t, ndom, res + 0);
+  k_fold_ordered<<<1, 256, 0, h->stream>>>(mdot_t, nyz, res + 1);
+  k_fold_ordered<<<1, 256, 0, h->stream>>>(rad_t, nyz, res + 2);
+  k_fold_ordered<<<1, 256, 0, h->stream>>>(tot_t, nyz, res + 3);
+  // scale height: the dynamo's per-radius fold (dynamo.zig:239), into a scratch row
+  DevState ds2 = h->ds;
+  ds2.scaleth = scaleth;
+  k_scale_height<<<nblk(gr.nx, SH_COLS), SH_WARPS * 32, 0, h->stream>>>(ds2);
+  k_init_beta_max<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam);
+  double hres[10], hsh = 0.0;
+  DevScalars z;
+  if ((st = sync_check(h, "scalars"))) return st;
+  cudaMemcpyAsync(hres, res, sizeof hres, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(&hsh, scaleth + ix_s, sizeof hsh, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(&z, h->dsc, sizeof z, cudaMemcpyDeviceToHost, h->stream);
+  if ((st = cuda_check(h, cudaStreamSynchronize(h->stream), "scalars"))) return st;
+  if (z.err) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "scalars: velocity conversion failed with status %d at cell %lld", z.err, z.err_cell);
+    return fail(h, z.err, buf);
+  }
+  unsigned long long counts[2];
+  memcpy(counts, hres + 8, sizeof counts);
+  double maxb = 0.0;
+  if (z.tsd_max_bits) memcpy(&maxb, &z.tsd_max_bits, 8);
+  out->t = h->t;
+  out->dt = dt;
+  out->nstep = h->nstep;
+  out->mass = hres[0];
+  out->mdot = -hres[1];
+  out->radlum = hres[2];
+  out->totallum = hres[3];
+  out->scaleheight = hsh;
+  out->max_pmag_ptot = maxb;
+  out->n_hd_fixup = (int64_t)counts[1];
+  out->n_radimp_fail = h->n_fail;
+  out->n_nan = (int64_t)counts[0];
+  out->n_floorguard = h->n_guard;
+  return KC_OK;
+}
+
 int kc_finish_init(kc_handle* h) {
   int st = kc_set_bc(h);
   if (st) return st;

@@ -1199,4 +1199,103 @@ __global__ void __launch_bounds__(128) k_init_beta_scale(DevState s, double gam,
   store_cell(s.u, nc, c, uu);
 }
 
+// ---- scalar diagnostics (koral/io/scalars.zig, koral/io/dump.zig:358) ---------
+// Each reduction writes its per-cell terms in the reference's serial loop order
+// and k_fold_ordered adds them in that order, so the sums are the serial ones.
+
+// per domain cell: the totalMass term (scalars.zig:78) at index
+// ix + nx (iy + ny iz), and the collectDiag counts (non-finite cells, hd flags)
+__global__ void __launch_bounds__(128) k_diag_cells(DevState s, double phifac, double* mass_terms,
+                                                    unsigned long long* counts) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  const Grid& g = s.gr.g;
+  double dx = cell_size(g, ix, 0), dy = cell_size(g, iy, 1), dz = cell_size(g, iz, 2) * phifac;
+  mass_terms[ix + s.gr.nx * (iy + s.gr.ny * iz)] = s.p[RHO * nc + c] * dx * dy * dz * s.cgc[10L * nc + c];
+  bool bad = false;
+  for (int iv = 0; iv < NV; ++iv)
+    if (!kmath::isfinite(s.p[iv * nc + c])) bad = true;
+  if (bad) atomicAdd(&counts[0], 1ULL);
+  if (s.flags[3 * nc + c] != 0) atomicAdd(&counts[1], 1ULL);
+}
+// the mdot terms through radial shell ix (scalars.zig:106), index iy + ny iz;
+// dzfac = 0 selects the 2D dphi = 2 pi
+__global__ void __launch_bounds__(128) k_diag_mdot(DevState s, DevScalars* sc, long ix, double dzfac, double* terms) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long ny = s.gr.ny;
+  if (t >= ny * s.gr.nz) return;
+  long iy = t % ny, iz = t / ny;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  double vcon[4] = {0.0, s.p[VX * nc + c], s.p[VY * nc + c], s.p[VZ * nc + c]}, ucon[4];
+  int e = convert(vcon, VELR, VEL4, geo, RECOMPUTE_UT, ucon);
+  if (e) {
+    set_err(sc, e, c);
+    terms[t] = 0.0;
+    return;
+  }
+  double rhouconr = s.p[RHO * nc + c] * ucon[1];
+  double dy = cell_size(s.gr.g, iy, 1);
+  double dz = dzfac == 0.0 ? 2.0 * KP_PI : cell_size(s.gr.g, iz, 2) * dzfac;
+  terms[t] = geo.gdet * rhouconr * dy * dz;
+}
+// the type-1 luminosity terms through radial shell ix in BL (scalars.zig:136):
+// gbl, dth, dph are the shell's BL geometry and cell widths, index iy + ny iz
+__global__ void __launch_bounds__(128) k_diag_lum(DevState s, DevScalars* sc, long ix, double gam, const Geom* gbl,
+                                                  const double* dth, const double* dph, double* rad_terms,
+                                                  double* tot_terms) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long ny = s.gr.ny;
+  if (t >= ny * s.gr.nz) return;
+  long iy = t % ny, iz = t / ny;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  double pp[NV];
+  load_cell(s.p, nc, c, pp);
+  Geom geo;
+  geom_cell(s, ix, iy, iz, geo);
+  const Geom& gb = gbl[t];
+  double jac[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) jac[i][j] = s.jbl[(long)(i * 4 + j) * nc + c];
+  int e = trans_pmhd_coco_j(pp, geo, gb, jac, pp);
+  if (!e) e = trans_prad_coco_j(pp, geo, gb, jac, pp);
+  double vcon[4] = {0.0, pp[VX], pp[VY], pp[VZ]}, ucon[4];
+  if (!e) e = convert(vcon, VELR, VEL4, gb, RECOMPUTE_UT, ucon);
+  if (e) {
+    set_err(sc, e, c);
+    rad_terms[t] = 0.0;
+    tot_terms[t] = 0.0;
+    return;
+  }
+  double rhour = pp[RHO] * ucon[1];
+  double tup[4][4], tij[4][4], rup[4][4], rij[4][4];
+  calc_tij(pp, gb, gam, tup);
+  lower_second(tup, gb, tij);
+  double trt = tij[1][0];
+  calc_rij(pp, gb, rup);
+  lower_second(rup, gb, rij);
+  double rrt = -rij[1][0];
+  if (rrt < 0.0) rrt = 0.0;
+  rad_terms[t] = gb.gdet * rrt * dth[t] * dph[t];
+  tot_terms[t] = gb.gdet * (rhour + trt + rrt) * dth[t] * dph[t];
+}
+// out[0] = ((0 + v[0]) + v[1]) + ... in index order: a block stages tiles in
+// shared memory, thread 0 adds them in order
+__global__ void __launch_bounds__(256) k_fold_ordered(const double* v, long n, double* out) {
+  __shared__ double tile[2048];
+  double acc = 0.0;
+  for (long k0 = 0; k0 < n; k0 += 2048) {
+    long m = n - k0 < 2048 ? n - k0 : 2048;
+    for (long k = threadIdx.x; k < m; k += blockDim.x) tile[k] = v[k0 + k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (long k = 0; k < m; ++k) acc += tile[k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = acc;
+}
+
 }  // namespace kc

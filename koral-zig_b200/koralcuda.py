@@ -122,6 +122,7 @@ def lib():
     L.kc_implicit_batch_noalloc.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
     L.kc_implicit_batch_device.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32, vp]
     L.kc_synth_implicit_cells.argtypes = [P(KcOptions), i64, ctypes.c_uint64, vp, vp, vp]
+    L.kc_scalars.argtypes = [vp, dbl, dbl, dbl, P(KcScalarRow)]
     L.kc_set_pass_timing.argtypes = [vp, i32]
     L.kc_get_pass_times.argtypes = [vp, vp, vp]
     L.kc_pass_name.argtypes = [i32]
@@ -136,7 +137,7 @@ def lib():
               "kc_set_precision", "kc_set_implicit_mode", "kc_set_guess", "kc_init_puffy", "kc_implicit_batch",
               "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
               "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc", "kc_implicit_batch_device",
-              "kc_synth_implicit_cells"]:
+              "kc_synth_implicit_cells", "kc_scalars"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -264,6 +265,12 @@ class Sim:
         dt = float("nan") if forced_dt is None else float(forced_dt)
         self._check(self._lib.kc_step(self._h, dt, ctypes.byref(info)))
         return info.dt
+
+    def scalars(self, dt=0.0, r_lum=5000.0, r_scale=15.0):
+        """dump.scalarRow (koral/io/dump.zig:383) at the current state."""
+        row = KcScalarRow()
+        self._check(self._lib.kc_scalars(self._h, dt, r_lum, r_scale, ctypes.byref(row)))
+        return {k: getattr(row, k) for k, _ in KcScalarRow._fields_}
 
     # ---- pass timers (koral/sim/timers.zig) and device plumbing -----------------
     def set_pass_timing(self, on):

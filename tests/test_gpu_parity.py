@@ -165,3 +165,36 @@ def test_forced_dt_steps_bitwise_from_c_state(name, mode):
         orc.step(float(z["dt"][k]))
     assert gpu.counters()["n_radimp_iters"] == orc.counters()["n_radimp_iters"]
     _assert_same_state(gpu, orc)
+
+
+def _scalars_equal(rg, ro):
+    for k in rg:
+        a, b = rg[k], ro[k]
+        if isinstance(a, float):
+            assert np.float64(a).view(np.uint64) == np.float64(b).view(np.uint64), (k, a, b)
+        else:
+            assert a == b, (k, a, b)
+
+
+def test_scalar_row_bitwise_vs_oracle_2d_after_steps():
+    """dump.scalarRow on the engine (ordered device folds) against the oracle's
+    serial loops, from the puffy_fast snapshot after 3 CFL steps."""
+    z, gpu, orc = _start("puffy_fast")
+    for _ in range(3):
+        gpu.step()
+        orc.step()
+    _scalars_equal(gpu.scalars(0.5, 5000.0, 15.0), orc.scalar_row(0.5, 5000.0, 15.0))
+    # a shell inside the domain for the luminosity (r_lum = 50)
+    _scalars_equal(gpu.scalars(0.0, 50.0, 30.0), orc.scalar_row(0.0, 50.0, 30.0))
+
+
+def test_scalar_row_bitwise_vs_oracle_3d():
+    kc = _kc()
+    grid, opt = kc.puffy_grid(24, 20, 8), kc.puffy_options()
+    gpu, orc = _pair(grid, opt)
+    gpu.initPuffy(1e-3, 1e-3, 7)
+    orc.init_puffy(1e-3, 1e-3, 7)
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    gpu.step()
+    orc.step()
+    _scalars_equal(gpu.scalars(0.0, 40.0, 15.0), orc.scalar_row(0.0, 40.0, 15.0))

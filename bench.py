@@ -293,6 +293,65 @@ def run_implicit(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_precision(args, rank, local):
+    """The mixed form (FP32 reconstruction, LAXF, flux-CT) against plain FP64 on
+    the same wedge and init, the mixed run forced to the FP64 run's dt sequence:
+    per-primitive field-scale error of the final state and the relative error of
+    the integrated mass, accretion rate (horizon), luminosity and scale height."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    kc = load_engine()
+    grid = kc.puffy_grid(args.nx, args.ny, args.nz)
+    out = {}
+    dts = []
+    names = ["rho", "uu", "vx", "vy", "vz", "entr", "b1", "b2", "b3", "ee", "fx", "fy", "fz"]
+    for form, mode in (("fp64", 0), ("mixed", 1), ("fp64_seeded", 0)):
+        sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode))
+        sim.initPuffy(1e-3, 1e-3, args.seed)
+        if form == "fp64_seeded":
+            # the FP64 run's own sensitivity: a 1e-15 relative seed on the conserved density
+            u = sim.u
+            u[:, 0] *= 1.0 + 1e-15 * np.random.default_rng(5).uniform(-1.0, 1.0, u.shape[0])
+            sim.set_cons(u)
+        stream = torch.cuda.ExternalStream(sim.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for k in range(args.steps):
+            if form == "fp64":
+                dts.append(sim.step())
+            else:
+                sim.step(dts[k])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[form] = {"p": sim.p, "scalars": sim.scalars(0.0, 5000.0, 15.0), "ms_per_step": ms / args.steps,
+                     "value": args.nx * args.ny * args.nz * args.steps / (ms / 1e3)}
+        sim.close()
+    b = out["fp64"]["p"]
+    ok = np.all(np.isfinite(b), axis=1)
+
+    def dev_of(form):
+        a = out[form]["p"]
+        d = np.abs(a[ok] - b[ok]).max(axis=0) / np.maximum(np.abs(b[ok]).max(axis=0), 1e-300)
+        r = {k: abs(out[form]["scalars"][k] / out["fp64"]["scalars"][k] - 1)
+             for k in ("mass", "mdot", "radlum", "totallum", "scaleheight")}
+        return d, r
+
+    dev, rel = dev_of("mixed")
+    dev_s, rel_s = dev_of("fp64_seeded")
+    line = {"metric": METRIC, "unit": UNIT, "workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz}, {args.steps} steps",
+            "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms_per_step"]},
+            "mixed": {"value": out["mixed"]["value"], "ms_per_step": out["mixed"]["ms_per_step"]},
+            "field_scale_error": dict(zip(names, dev.tolist())), "integrated_rel_error": rel,
+            "fp64_seed_1e-15": {"field_scale": dict(zip(names, dev_s.tolist())), "integrated_rel": rel_s},
+            "scalars_fp64": out["fp64"]["scalars"], "scalars_mixed": out["mixed"]["scalars"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -305,8 +364,9 @@ def main():
     ap.add_argument("--seed", type=int, default=20250)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="step", choices=["step", "implicit"],
-                    help="step: the RK2IMEX step on the wedge; implicit: the batched implicit-solve microbenchmark")
+    ap.add_argument("--workload", default="step", choices=["step", "implicit", "precision"],
+                    help="step: the RK2IMEX step on the wedge; implicit: the batched implicit-solve microbenchmark; "
+                         "precision: mixed vs plain FP64 error study on the wedge")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
     ap.add_argument("--implicit-mode", default="per-cell", choices=["per-cell", "compacting"],
                     help="implicit solve form: one thread per cell, or the persistent lane-refilling state machine")
@@ -318,6 +378,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.workload == "implicit":
         return run_implicit(args, rank, world, local)
+    if args.workload == "precision":
+        return run_precision(args, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -401,7 +401,8 @@ void launch_face_fluxes(kc_handle* h) {
     long n1 = dims[c1] > 1 ? dims[c1] + 2 : dims[c1];
     long n = (dims[dim] + 1) * n0 * n1;
     ++h->n_launch;
-    k_face_flux<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
+    if (h->opt.precision == KC_MIXED) k_face_flux<true><<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
+    else k_face_flux<false><<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
   }
 }
 
@@ -410,9 +411,11 @@ void launch_flux_ct(kc_handle* h) {
   long n = (long)(gr.nx + 1) * (gr.ny + 1) * (gr.nz + 1);
   PassScope ps(h, KC_PASS_FLUXCT);
   ++h->n_launch;
-  k_ct_emf<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  if (h->opt.precision == KC_MIXED) k_ct_emf<float><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  else k_ct_emf<double><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
   ++h->n_launch;
-  k_ct_rebuild<<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  if (h->opt.precision == KC_MIXED) k_ct_rebuild<float><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  else k_ct_rebuild<double><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
 }
 
 void launch_op_explicit(kc_handle* h, double dtin) {
@@ -1000,7 +1003,7 @@ int kc_debug_get_array(kc_handle* h, int which, double* out) {
 
 int kc_set_precision(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (mode != KC_PLAIN_FP64) return fail(h, KC_ERR_INVALID_CONFIG, "precision mode not built");
+  if (mode != KC_PLAIN_FP64 && mode != KC_MIXED) return fail(h, KC_ERR_INVALID_CONFIG, "unknown precision mode");
   h->opt.precision = mode;
   return KC_OK;
 }

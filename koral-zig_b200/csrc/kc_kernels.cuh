@@ -6,6 +6,7 @@
 #pragma once
 #include "kc_dev.cuh"
 #include "kc_implicit_sm.cuh"
+#include "kc_mixed.cuh"
 
 namespace kc {
 
@@ -650,6 +651,8 @@ __device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, 
   }
   return E_OK;
 }
+// MIXED: the reconstruction and the LAXF combination in FP32 (kc_mixed.cuh)
+template <bool MIXED>
 __global__ void __launch_bounds__(128) k_face_flux(DevState s, DevScalars* sc, FluxArgs a, int dim) {
   long n = dim == 0 ? s.gr.nx : dim == 1 ? s.gr.ny : s.gr.nz;
   int c0d = dim == 0 ? 1 : 0, c1d = dim == 2 ? 1 : 2;
@@ -691,10 +694,15 @@ __global__ void __launch_bounds__(128) k_face_flux(DevState s, DevScalars* sc, F
   for (int iv = 0; iv < NV; ++iv) {
     double v[6];
     for (int k = 0; k < 6; ++k) v[k] = s.p[iv * nc + cst[k]];
-    Faces fl = reconstruct(RECON_PPM, v, dxs, a.theta);          // cell f-1: right face value
-    Faces fr = reconstruct(RECON_PPM, v + 1, dxs + 1, a.theta);  // cell f: left face value
-    pL[iv] = fl.right;
-    pR[iv] = fr.left;
+    if (MIXED) {
+      pL[iv] = recon_ppm_mixed(v, dxs).right;
+      pR[iv] = recon_ppm_mixed(v + 1, dxs + 1).left;
+    } else {
+      Faces fl = reconstruct(RECON_PPM, v, dxs, a.theta);          // cell f-1: right face value
+      Faces fr = reconstruct(RECON_PPM, v + 1, dxs + 1, a.theta);  // cell f: left face value
+      pL[iv] = fl.right;
+      pR[iv] = fr.left;
+    }
   }
   Geom geo;
   geom_face(s, cf[0], cf[1], cf[2], dim, geo);
@@ -712,7 +720,9 @@ __global__ void __launch_bounds__(128) k_face_flux(DevState s, DevScalars* sc, F
   double* out = s.flb[dim];
   long nfd = s.nf[dim];
 #pragma unroll
-  for (int iv = 0; iv < NV; ++iv) out[iv * nfd + fi] = laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
+  for (int iv = 0; iv < NV; ++iv)
+    out[iv * nfd + fi] = MIXED ? laxf_f(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag)
+                               : laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
 }
 
 // ---- flux-CT (koral/sim/ct.zig:38) --------------------------------------------
@@ -720,61 +730,65 @@ __device__ __forceinline__ long pin(long n, long i) { return n == 1 ? 0 : i; }
 __device__ __forceinline__ double flbv(const DevState& s, int dim, int iv, long ix, long iy, long iz) {
   return s.flb[dim][(long)iv * s.nf[dim] + face_index(s.gr, dim, ix, iy, iz)];
 }
+// R: the arithmetic type of the corner averages (float in the mixed form)
+template <class R>
 __global__ void k_ct_emf(DevState s) {
   long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (nx + 1) * (ny + 1) * (nz + 1)) return;
   long ix = t % (nx + 1), q = t / (nx + 1), iy = q % (ny + 1), iz = q / (ny + 1);
-  double coef1 = (ny > 1 && nz > 1) ? 0.25 : 0.5;
-  double coef2 = (nx > 1 && nz > 1) ? 0.25 : 0.5;
-  double coef3 = (nx > 1 && ny > 1) ? 0.25 : 0.5;
+  R coef1 = (ny > 1 && nz > 1) ? R(0.25) : R(0.5);
+  R coef2 = (nx > 1 && nz > 1) ? R(0.25) : R(0.5);
+  R coef3 = (nx > 1 && ny > 1) ? R(0.25) : R(0.5);
+  auto F = [&](int dim, int iv, long jx, long jy, long jz) { return (R)flbv(s, dim, iv, jx, jy, jz); };
   if (ny > 1 || nz > 1) {
-    double sm = 0.0;
-    if (ny > 1) sm += flbv(s, 1, B3, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 1, B3, pin(nx, ix), pin(ny, iy), pin(nz, iz - 1));
-    if (nz > 1) sm -= flbv(s, 2, B2, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 2, B2, pin(nx, ix), pin(ny, iy - 1), pin(nz, iz));
-    s.emf[0][t] = coef1 * sm;
+    R sm = R(0);
+    if (ny > 1) sm += F(1, B3, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + F(1, B3, pin(nx, ix), pin(ny, iy), pin(nz, iz - 1));
+    if (nz > 1) sm -= F(2, B2, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + F(2, B2, pin(nx, ix), pin(ny, iy - 1), pin(nz, iz));
+    s.emf[0][t] = (double)(coef1 * sm);
   } else {
     s.emf[0][t] = 0.0;
   }
   if (nx > 1 || nz > 1) {
-    double sm = 0.0;
-    if (nz > 1) sm += flbv(s, 2, B1, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 2, B1, pin(nx, ix - 1), pin(ny, iy), pin(nz, iz));
-    if (nx > 1) sm -= flbv(s, 0, B3, ix, pin(ny, iy), pin(nz, iz)) + flbv(s, 0, B3, ix, pin(ny, iy), pin(nz, iz - 1));
-    s.emf[1][t] = coef2 * sm;
+    R sm = R(0);
+    if (nz > 1) sm += F(2, B1, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + F(2, B1, pin(nx, ix - 1), pin(ny, iy), pin(nz, iz));
+    if (nx > 1) sm -= F(0, B3, ix, pin(ny, iy), pin(nz, iz)) + F(0, B3, ix, pin(ny, iy), pin(nz, iz - 1));
+    s.emf[1][t] = (double)(coef2 * sm);
   } else {
     s.emf[1][t] = 0.0;
   }
   if (nx > 1 || ny > 1) {
-    double sm = 0.0;
-    if (nx > 1) sm += flbv(s, 0, B2, ix, pin(ny, iy), pin(nz, iz)) + flbv(s, 0, B2, ix, pin(ny, iy - 1), pin(nz, iz));
-    if (ny > 1) sm -= flbv(s, 1, B1, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + flbv(s, 1, B1, pin(nx, ix - 1), pin(ny, iy), pin(nz, iz));
-    s.emf[2][t] = coef3 * sm;
+    R sm = R(0);
+    if (nx > 1) sm += F(0, B2, ix, pin(ny, iy), pin(nz, iz)) + F(0, B2, ix, pin(ny, iy - 1), pin(nz, iz));
+    if (ny > 1) sm -= F(1, B1, pin(nx, ix), pin(ny, iy), pin(nz, iz)) + F(1, B1, pin(nx, ix - 1), pin(ny, iy), pin(nz, iz));
+    s.emf[2][t] = (double)(coef3 * sm);
   } else {
     s.emf[2][t] = 0.0;
   }
 }
+template <class R>
 __global__ void k_ct_rebuild(DevState s) {
   long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (nx + 1) * (ny + 1) * (nz + 1)) return;
   long ix = t % (nx + 1), q = t / (nx + 1), iy = q % (ny + 1), iz = q / (ny + 1);
-  auto E = [&](int comp, long jx, long jy, long jz) { return s.emf[comp - 1][(jz * (ny + 1) + jy) * (nx + 1) + jx]; };
+  auto E = [&](int comp, long jx, long jy, long jz) { return (R)s.emf[comp - 1][(jz * (ny + 1) + jy) * (nx + 1) + jx]; };
   if (nx > 1 && iy < ny && iz < nz) {
     long fi = face_index(s.gr, 0, ix, iy, iz), nf = s.nf[0];
     s.flb[0][B1 * nf + fi] = 0.0;
-    s.flb[0][B2 * nf + fi] = 0.5 * (E(3, ix, iy, iz) + E(3, ix, iy + 1, iz));
-    s.flb[0][B3 * nf + fi] = -0.5 * (E(2, ix, iy, iz) + E(2, ix, iy, iz + 1));
+    s.flb[0][B2 * nf + fi] = (double)(R(0.5) * (E(3, ix, iy, iz) + E(3, ix, iy + 1, iz)));
+    s.flb[0][B3 * nf + fi] = (double)(R(-0.5) * (E(2, ix, iy, iz) + E(2, ix, iy, iz + 1)));
   }
   if (ny > 1 && ix < nx && iz < nz) {
     long fi = face_index(s.gr, 1, ix, iy, iz), nf = s.nf[1];
-    s.flb[1][B1 * nf + fi] = -0.5 * (E(3, ix, iy, iz) + E(3, ix + 1, iy, iz));
+    s.flb[1][B1 * nf + fi] = (double)(R(-0.5) * (E(3, ix, iy, iz) + E(3, ix + 1, iy, iz)));
     s.flb[1][B2 * nf + fi] = 0.0;
-    s.flb[1][B3 * nf + fi] = 0.5 * (E(1, ix, iy, iz) + E(1, ix, iy, iz + 1));
+    s.flb[1][B3 * nf + fi] = (double)(R(0.5) * (E(1, ix, iy, iz) + E(1, ix, iy, iz + 1)));
   }
   if (nz > 1 && ix < nx && iy < ny) {
     long fi = face_index(s.gr, 2, ix, iy, iz), nf = s.nf[2];
-    s.flb[2][B1 * nf + fi] = 0.5 * (E(2, ix, iy, iz) + E(2, ix + 1, iy, iz));
-    s.flb[2][B2 * nf + fi] = -0.5 * (E(1, ix, iy, iz) + E(1, ix, iy + 1, iz));
+    s.flb[2][B1 * nf + fi] = (double)(R(0.5) * (E(2, ix, iy, iz) + E(2, ix + 1, iy, iz)));
+    s.flb[2][B2 * nf + fi] = (double)(R(-0.5) * (E(1, ix, iy, iz) + E(1, ix, iy + 1, iz)));
     s.flb[2][B3 * nf + fi] = 0.0;
   }
 }

@@ -266,6 +266,10 @@ class Sim:
         self._check(self._lib.kc_step(self._h, dt, ctypes.byref(info)))
         return info.dt
 
+    def set_precision(self, mode):
+        """KC_PLAIN_FP64 or KC_MIXED (FP32 reconstruction, LAXF and flux-CT)."""
+        self._check(self._lib.kc_set_precision(self._h, mode))
+
     def scalars(self, dt=0.0, r_lum=5000.0, r_scale=15.0):
         """dump.scalarRow (koral/io/dump.zig:383) at the current state."""
         row = KcScalarRow()

@@ -87,11 +87,11 @@ KC_HDM void invert4(const double a_in[4][4], double inv[4][4]) {
 KC_HDN int apply_constraints(double pp[NV], double uu[NV], const double uu0[NV], const Geom& g, double gam,
                              const RadParams& rad, const ImplicitParams& ip, int whichprim) {
   double gdetu = g.gdet;
-  double gdetu_inv = 1.0 / gdetu;
+  double gdetu_inv = kmath::div(1.0, gdetu);
   if (whichprim == PRIM_MHD) {
     double ucon[4], ucov[4];
     ucon_ucov_from_prims(pp[VX], pp[VY], pp[VZ], g, ucon, ucov);
-    pp[RHO] = uu0[RHO] * gdetu_inv / ucon[0];
+    pp[RHO] = kmath::div(uu0[RHO] * gdetu_inv, ucon[0]);
     pp[ENTR] = s_from_u(pp[RHO], pp[UU], gam);
     p2u_mhd(pp, uu, g, gam);
     for (int k = 0; k < 4; ++k) uu[EE + k] = uu0[EE + k] - (uu[UU + k] - uu0[UU + k]);
@@ -125,7 +125,7 @@ KC_HDN double implicit_residual(const double uu[NV], const double pp[NV], const 
   double tgas = st.tgas;
   double ehat0 = st0.ehat;
   double ehat = st.ehat;
-  double dtau = dt / st.ucon[0];
+  double dtau = kmath::div(dt, st.ucon[0]);
   double giff[4], gilab[4], gi[4];
   calc_gi_from_state(st, pp[VX], pp[VY], pp[VZ], g, op, false, giff, gilab);
   lower_vec(gilab, g, gi);
@@ -134,16 +134,16 @@ KC_HDN double implicit_residual(const double uu[NV], const double pp[NV], const 
     for (int k = 1; k < 4; ++k) {
       f[k] = uu[UU + k] - uu0[UU + k] - dt * gdetu * gi[k];
       err[k] = (kmath::fabs(f[k]) > small)
-                   ? kmath::fabs(f[k]) / (1.0e-20 * uu[UU] + kmath::fabs(uu[UU + k]) + kmath::fabs(uu0[UU + k]) +
-                                          kmath::fabs(dt * gdetu * gi[k]))
+                   ? kmath::div(kmath::fabs(f[k]), (1.0e-20 * uu[UU] + kmath::fabs(uu[UU + k]) + kmath::fabs(uu0[UU + k]) +
+                                          kmath::fabs(dt * gdetu * gi[k])))
                    : 0.0;
     }
   } else {
     for (int k = 1; k < 4; ++k) {
       f[k] = uu[EE + k] - uu0[EE + k] + dt * gdetu * gi[k];
       err[k] = (kmath::fabs(f[k]) > small)
-                   ? kmath::fabs(f[k]) / (1.0e-20 * uu[EE] + kmath::fabs(uu[EE + k]) + kmath::fabs(uu0[EE + k]) +
-                                          kmath::fabs(dt * gdetu * gi[k]))
+                   ? kmath::div(kmath::fabs(f[k]), (1.0e-20 * uu[EE] + kmath::fabs(uu[EE + k]) + kmath::fabs(uu0[EE + k]) +
+                                          kmath::fabs(dt * gdetu * gi[k])))
                    : 0.0;
     }
   }
@@ -151,28 +151,28 @@ KC_HDN double implicit_residual(const double uu[NV], const double pp[NV], const 
     if (whichprim == PRIM_RAD) {
       f[0] = uu[EE] - uu0[EE] + dt * gdetu * gi[0];
       err[0] = (kmath::fabs(f[0]) > small)
-                   ? kmath::fabs(f[0]) / (kmath::fabs(uu[EE]) + kmath::fabs(uu0[EE]) + kmath::fabs(dt * gdetu * gi[0]))
+                   ? kmath::div(kmath::fabs(f[0]), (kmath::fabs(uu[EE]) + kmath::fabs(uu0[EE]) + kmath::fabs(dt * gdetu * gi[0])))
                    : 0.0;
     } else {
       f[0] = uu[UU] - uu0[UU] - dt * gdetu * gi[0];
       err[0] = (kmath::fabs(f[0]) > small)
-                   ? kmath::fabs(f[0]) / (kmath::fabs(uu[UU]) + kmath::fabs(uu0[UU]) + kmath::fabs(dt * gdetu * gi[0]))
+                   ? kmath::div(kmath::fabs(f[0]), (kmath::fabs(uu[UU]) + kmath::fabs(uu0[UU]) + kmath::fabs(dt * gdetu * gi[0])))
                    : 0.0;
     }
   } else {
     if (whicheq == EQ_ENERGY) {
       if (whichprim == PRIM_RAD) {
         f[0] = ehat - ehat0 + dtau * giff[0];
-        err[0] = kmath::fabs(f[0]) / (kmath::fabs(ehat) + kmath::fabs(ehat0) + kmath::fabs(dtau * giff[0]));
+        err[0] = kmath::div(kmath::fabs(f[0]), (kmath::fabs(ehat) + kmath::fabs(ehat0) + kmath::fabs(dtau * giff[0])));
       } else {
         f[0] = pp[UU] - st0.uint_ - dtau * giff[0];
-        err[0] = kmath::fabs(f[0]) / (kmath::fabs(pp[UU]) + kmath::fabs(st0.uint_) + kmath::fabs(dtau * giff[0]));
+        err[0] = kmath::div(kmath::fabs(f[0]), (kmath::fabs(pp[UU]) + kmath::fabs(st0.uint_) + kmath::fabs(dtau * giff[0])));
       }
     } else {
       double s0 = st0.sgas;
       double s = st.sgas;
       f[0] = tgas * (s - s0) - dtau * giff[0];
-      err[0] = kmath::fabs(f[0]) / (kmath::fabs(tgas * s) + kmath::fabs(tgas * s0) + kmath::fabs(dtau * giff[0]));
+      err[0] = kmath::div(kmath::fabs(f[0]), (kmath::fabs(tgas * s) + kmath::fabs(tgas * s0) + kmath::fabs(dtau * giff[0])));
     }
   }
   double err0 = 0.0;
@@ -194,12 +194,12 @@ KC_HDM double f1d_err(double xxx, const double pp0[NV], double dtau, const Geom&
   double pp[NV];
   for (int i = 0; i < NV; ++i) pp[i] = pp0[i];
   pp[UU] = ugas;
-  pp[EE] = ehat / ratio;
+  pp[EE] = kmath::div(ehat, ratio);
   RadState st;
   fill_rad_state(pp, g, gam, op, false, st);
   double giff[4], gilab[4];
   calc_gi_from_state(st, pp[VX], pp[VY], pp[VZ], g, op, false, giff, gilab);
-  if (whichprim == PRIM_RAD) return ehat - pp0[EE] / ratio + dtau * giff[0];
+  if (whichprim == PRIM_RAD) return ehat - kmath::div(pp0[EE], ratio) + dtau * giff[0];
   return ugas - pp0[UU] - dtau * giff[0];
 }
 
@@ -207,26 +207,26 @@ KC_HDM double f1d_err(double xxx, const double pp0[NV], double dtau, const Geom&
 KC_HDN int solve_1d_prim(const double pp00[NV], const RadState& st00, const Geom& g, double dt, double gam,
                          const OpacParams& op, double pp0out[NV]) {
   double ehat = st00.ehat;
-  double dtau = dt / st00.ucon[0];
+  double dtau = kmath::div(dt, st00.ucon[0]);
   double totenergy = ehat + pp00[UU];
   int whichprim = (ehat < 1.0e-3 * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
   double tgas = st00.tgas;
-  double ratio = ehat / pp00[EE];
+  double ratio = kmath::div(ehat, pp00[EE]);
   const double fac = 3.0;
   const double fac1 = fac + 1.0;
   double pp_uu = pp00[UU];
   double pp_ee = pp00[EE];
   if (tgas > 1.0e14) {
-    pp_uu = pp00[UU] * 1.0e14 / tgas;
-    pp_ee = (totenergy - pp_uu) / ratio;
+    pp_uu = kmath::div(pp00[UU] * 1.0e14, tgas);
+    pp_ee = kmath::div((totenergy - pp_uu), ratio);
   }
   double xlo, xhi;
   if (whichprim == PRIM_MHD) {
-    xlo = pp_uu / 1.05;
-    xhi = kmath::fmin(pp_uu * 1.05, (pp_uu + fac * totenergy) / fac1);
+    xlo = kmath::div(pp_uu, 1.05);
+    xhi = kmath::fmin(pp_uu * 1.05, kmath::div((pp_uu + fac * totenergy), fac1));
   } else {
-    xlo = pp_ee / 1.05;
-    xhi = kmath::fmin(pp_ee * 1.05, (pp_ee + fac * totenergy / ratio) / fac1);
+    xlo = kmath::div(pp_ee, 1.05);
+    xhi = kmath::fmin(pp_ee * 1.05, kmath::div((pp_ee + kmath::div(fac * totenergy, ratio)), fac1));
   }
   double errlo = f1d_err(xlo, pp00, dtau, g, gam, op, whichprim, totenergy, ratio);
   double errhi = f1d_err(xhi, pp00, dtau, g, gam, op, whichprim, totenergy, ratio);
@@ -243,8 +243,8 @@ KC_HDN int solve_1d_prim(const double pp00[NV], const RadState& st00, const Geom
     } else {
       xlo = xhi;
       errlo = errhi;
-      if (whichprim == PRIM_RAD) xhi = kmath::fmin(xhi * fac, (xhi + fac * totenergy / ratio) / fac1);
-      else xhi = kmath::fmin(xhi * fac, (xhi + fac * totenergy) / fac1);
+      if (whichprim == PRIM_RAD) xhi = kmath::fmin(xhi * fac, kmath::div((xhi + kmath::div(fac * totenergy, ratio)), fac1));
+      else xhi = kmath::fmin(xhi * fac, kmath::div((xhi + fac * totenergy), fac1));
       errhi = f1d_err(xhi, pp00, dtau, g, gam, op, whichprim, totenergy, ratio);
     }
     if (kmath::isnan(errlo) || kmath::isnan(errhi)) iter = maxiter;
@@ -270,7 +270,7 @@ KC_HDN int solve_1d_prim(const double pp00[NV], const RadState& st00, const Geom
       for (int i = 0; i < NV; ++i) pp0out[i] = pp00[i];
       return -1;
     }
-    if (!(kmath::fabs((xhi - xlo) / xmid) > conv)) break;
+    if (!(kmath::fabs(kmath::div((xhi - xlo), xmid)) > conv)) break;
   }
   for (int i = 0; i < NV; ++i) pp0out[i] = pp00[i];
   if (whichprim == PRIM_RAD) {
@@ -278,7 +278,7 @@ KC_HDN int solve_1d_prim(const double pp00[NV], const RadState& st00, const Geom
     pp0out[UU] = totenergy - xmid * ratio;
   } else {
     pp0out[UU] = xmid;
-    pp0out[EE] = (totenergy - xmid) / ratio;
+    pp0out[EE] = kmath::div((totenergy - xmid), ratio);
   }
   return 0;
 }
@@ -286,7 +286,7 @@ KC_HDN int solve_1d_prim(const double pp00[NV], const RadState& st00, const Geom
 // one-sided FD step of Jacobian column j (implicit.zig:586)
 KC_HD double fd_del(int j, double sign, const double ppp[NV], int sh, double eps, const Geom& g) {
   if (j == 0) return sign * eps * ppp[sh];
-  double veleps = eps * my_sign(ppp[j + sh]) * kmath::fmax(1.0e-8 / kmath::sqrt(g.gg[j][j]), kmath::fabs(ppp[j + sh]));
+  double veleps = eps * my_sign(ppp[j + sh]) * kmath::fmax(kmath::div(1.0e-8, kmath::sqrt(g.gg[j][j])), kmath::fabs(ppp[j + sh]));
   return (ppp[j + sh] >= 0.0) ? sign * veleps : -sign * veleps;
 }
 
@@ -350,7 +350,7 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
         fill_rad_state(pp, g, gam, op, !slim, state);
         if (ip.lag_opac) lag_opac(state, state00);
         implicit_residual(uu, pp, state, uu00, state00, dt, g, op, whichprim, whicheq, whichframe, f2);
-        for (int i = 0; i < 4; ++i) jac[i][j] = (f2[i] - f1[i]) / del;
+        for (int i = 0; i < 4; ++i) jac[i][j] = kmath::div((f2[i] - f1[i]), del);
         pp[j + sh] = ppp[j + sh];
         break;
       }
@@ -362,7 +362,7 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
     if (ip.scale_jacobian) {
       for (int j = 0; j < 4; ++j) {
         if (scalevec[j] == 0.0) scalevec[j] = 1.0;
-        invscalevec[j] = 1.0 / scalevec[j];
+        invscalevec[j] = kmath::div(1.0, scalevec[j]);
       }
       for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j)
@@ -383,18 +383,18 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
       fill_rad_state(pp, g, gam, op, !slim, state);
       if (ip.lag_opac) lag_opac(state, state00);
       bool okcheck = false;
-      double edenmin = ppp[sh] / ip.max_en_change_down;
+      double edenmin = kmath::div(ppp[sh], ip.max_en_change_down);
       double edenmax = ppp[sh] * ip.max_en_change_up;
       if (xxx[0] > edenmin && xxx[0] < edenmax && fret >= -1) okcheck = true;
       double tgasold = t_from_urho(op.c, ppp[UU], ppp[RHO], gam);
       double tgasnew = t_from_urho(op.c, pp[UU], pp[RHO], gam);
-      if (okcheck && (tgasnew > tgasold * ip.max_tgas_change || tgasnew < tgasold / ip.max_tgas_change)) okcheck = false;
+      if (okcheck && (tgasnew > tgasold * ip.max_tgas_change || tgasnew < kmath::div(tgasold, ip.max_tgas_change))) okcheck = false;
       double tradnew = lte_T_from_E(op.c, pp[EE]);
       double tradold = lte_T_from_E(op.c, ppp[EE]);
-      if (okcheck && (tradnew > tradold * ip.max_trad_change || tradnew < tradold / ip.max_trad_change)) okcheck = false;
+      if (okcheck && (tradnew > tradold * ip.max_trad_change || tradnew < kmath::div(tradold, ip.max_trad_change))) okcheck = false;
       if (okcheck) break;
       if (xxx[0] <= 0.0) {
-        xiapp *= ppp[sh] / (ppp[sh] + kmath::fabs(xxx[0]));
+        xiapp *= kmath::div(ppp[sh], (ppp[sh] + kmath::fabs(xxx[0])));
         xiapp *= 1.0e-1;
       } else {
         xiapp /= ip.damping_factor;
@@ -406,10 +406,10 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
     }
     if (!failed) {
       double f3[4];
-      f3[0] = kmath::fabs((pp[sh] - ppp[sh]) / ppp[sh]);
+      f3[0] = kmath::fabs(kmath::div((pp[sh] - ppp[sh]), ppp[sh]));
       for (int i = 1; i < 4; ++i) {
         f3[i] = pp[i + sh] - ppp[i + sh];
-        f3[i] = kmath::fabs(f3[i] / kmath::fmax(ip.eps, kmath::fabs(ppp[i + sh])));
+        f3[i] = kmath::fabs(kmath::div(f3[i], kmath::fmax(ip.eps, kmath::fabs(ppp[i + sh]))));
       }
       double convrel = (whicheq == EQ_ENTROPY) ? ip.convrelentr : ip.convrel;
       double convrelerr = (whicheq == EQ_ENTROPY) ? ip.convrelentrerr : ip.convrelerr;

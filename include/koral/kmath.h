@@ -101,13 +101,23 @@ KC_HD double fabs(double x) { return from_bits(to_bits(x) & 0x7fffffffffffffffUL
 KC_HD double copysign(double x, double s) {
   return from_bits((to_bits(x) & 0x7fffffffffffffffULL) | (to_bits(s) & 0x8000000000000000ULL));
 }
-KC_HD double sqrt(double x) {
+// Out of line on the device (one copy of the IEEE square-root sequence per
+// kernel instead of one per call site): the solver kernels are bound by
+// instruction fetch, and their code size is what matters there.
+KC_HDN double sqrt(double x) {
 #if defined(__CUDA_ARCH__)
   return __dsqrt_rn(x);
 #else
   return __builtin_sqrt(x);
 #endif
 }
+// IEEE double division a / b through one out-of-line copy of the divide
+// sequence. The opacity, four-force and implicit-solver code divides through
+// this: their kernels are bound by instruction fetch (the solve's call graph
+// is far larger than the instruction cache), and an inline double divide is
+// ~30 instructions at every site. The result is the same correctly rounded
+// quotient as `a / b`.
+KC_HDN double div(double a, double b) { return a / b; }
 // Zig's @min/@max on floats: the non-NaN operand wins (LLVM minnum/maxnum).
 KC_HD double fmin(double a, double b) {
   if (a != a) return b;

@@ -64,12 +64,12 @@ KC_HD double lte_E_from_T(const Consts& c, double t) { return c.four_sigmarad * 
 // C calc_PEQ_Tfromurho (thermo.zig:165)
 KC_HD double t_from_urho(const Consts& c, double uint_, double rho, double gam) {
   double p = uint_ * (gam - 1.0);
-  return c.mugas_mp_over_kb * p / rho;
+  return kmath::div(c.mugas_mp_over_kb * p, rho);
 }
 // C calc_PEQ_ufromTrho (thermo.zig:176)
 KC_HD double u_from_trho(const Consts& c, double t, double rho, double gam) {
   double p = c.kb_over_mugas_mp * rho * t;
-  return p / (gam - 1.0);
+  return kmath::div(p, (gam - 1.0));
 }
 struct Temps {
   double tgas, te, ti;
@@ -110,19 +110,19 @@ KC_HDN Opac calc_opacities(const Consts& c, const Channels& ch, double rho, doub
   double kappagassyn = 0, kapparadsyn = 0, kapparadnumsyn = 0, kapparadsynross = 0, kappagassynross = 0;
   if (ch.bremsstrahlung) {
     double mfrac = 1.0 - c.hfrac - c.hefrac;
-    double emis_ff = 1.4e-27 * nethcgs * ((c.hfrac + c.hefrac + c.z2diva_mean * mfrac) / c.m_proton_cgs) * rt_te * 1.2 *
+    double emis_ff = 1.4e-27 * nethcgs * (kmath::div((c.hfrac + c.hefrac + c.z2diva_mean * mfrac), c.m_proton_cgs)) * rt_te * 1.2 *
                      (1.0 + 4.4e-10 * te);
-    kappagasff = c.kappacgs2gu * (emis_ff / bbenergy) * rho;
+    kappagasff = c.kappacgs2gu * (kmath::div(emis_ff, bbenergy)) * rho;
     if (want_rad) {
-      double zeta = trad / te;
-      double zeta_inv = 1.0 / zeta;
+      double zeta = kmath::div(trad, te);
+      double zeta_inv = kmath::div(1.0, zeta);
       double zeta_inv_3 = zeta_inv * zeta_inv * zeta_inv;
       kapparadff = kappagasff * kmath::log1p(1.6 * zeta) * c.one_over_log_2p6 * zeta_inv_3;
       double zeta_root5 = kmath::pow(zeta, 0.2);
-      double zeta_root5_inv_4 = 1.0 / (zeta_root5 * zeta_root5 * zeta_root5 * zeta_root5);
+      double zeta_root5_inv_4 = kmath::div(1.0, (zeta_root5 * zeta_root5 * zeta_root5 * zeta_root5));
       double zeta_root5_inv_3 = zeta_root5 * zeta_root5_inv_4;
       double scale_pla_ros_ff =
-          14.12 / (432.7 - 106.8 * zeta_root5_inv_3 + 43.17 * zeta_root5_inv_4 + 57.88 * zeta_inv);
+          kmath::div(14.12, (432.7 - 106.8 * zeta_root5_inv_3 + 43.17 * zeta_root5_inv_4 + 57.88 * zeta_inv));
       kapparadffross = kappagasff * scale_pla_ros_ff * zeta_inv_3;
     }
     if (want_full) kappagasffross = kappagasff * 0.0330;
@@ -132,46 +132,46 @@ KC_HDN Opac calc_opacities(const Consts& c, const Channels& ch, double rho, doub
     double tc_n = 5.07783e9;
     double trad_syn = trad;
     if (bridge) {
-      double trad_lim = kmath::pow(tradbb, 4.0 / 3.0) / kmath::pow(te, 1.0 / 3.0);
+      double trad_lim = kmath::div(kmath::pow(tradbb, 4.0 / 3.0), kmath::pow(te, 1.0 / 3.0));
       trad_syn = (trad < trad_lim) ? trad_lim : trad;
     }
-    double emis_synchro = 3.61e-34 * (nethcgs / rhocgs) * te * te * bmagcgs * bmagcgs;
-    kappagassyn = c.kappacgs2gu * (emis_synchro / bbenergy) * rho;
+    double emis_synchro = 3.61e-34 * (kmath::div(nethcgs, rhocgs)) * te * te * bmagcgs * bmagcgs;
+    kappagassyn = c.kappacgs2gu * (kmath::div(emis_synchro, bbenergy)) * rho;
     if (want_rad) {
       double nu_mbsyn = 1.19e-13 * te * te;
-      double zbr = c.k_boltz_cgs * trad_syn / c.h_cgs / nu_mbsyn;
+      double zbr = kmath::div(kmath::div(c.k_boltz_cgs * trad_syn, c.h_cgs), nu_mbsyn);
       double zeta_a_denom_rad =
           1.79 * kmath::cbrt(zbr * zbr * zbr * zbr * zbr * bmagcgs * bmagcgs * bmagcgs * bmagcgs) +
           1.35 * kmath::cbrt(zbr * zbr * zbr * zbr * zbr * zbr * zbr * bmagcgs * bmagcgs) + 0.248 * zbr * zbr * zbr;
-      double ia_by_b_rad = bmagcgs * bmagcgs / zeta_a_denom_rad;
+      double ia_by_b_rad = kmath::div(bmagcgs * bmagcgs, zeta_a_denom_rad);
       double te5 = te * te * te * te * te;
-      kapparadsyn = c.kappacgs2gu * (2.13e39 * (nethcgs / rhocgs) / te5 * ia_by_b_rad) * rho;
+      kapparadsyn = c.kappacgs2gu * (kmath::div(2.13e39 * (kmath::div(nethcgs, rhocgs)), te5) * ia_by_b_rad) * rho;
       if (bridge)
         kapparadsyn += c.kappacgs2gu *
-                       (2.35869e-21 * (nethcgs / rhocgs) * (bmagcgs * bmagcgs) / (trad_syn * trad_syn * trad_syn)) * rho;
+                       (kmath::div(2.35869e-21 * (kmath::div(nethcgs, rhocgs)) * (bmagcgs * bmagcgs), (trad_syn * trad_syn * trad_syn))) * rho;
       if (want_full) {
         double zeta_a_denom_num = (0.025 * kmath::cbrt(zbr * zbr * zbr * zbr * bmagcgs * bmagcgs) +
                                    0.169 * kmath::cbrt(zbr * zbr * zbr * zbr * zbr * bmagcgs) + 0.287 * zbr * zbr);
-        double ia_by_b_num = bmagcgs / zeta_a_denom_num;
-        kapparadnumsyn = c.kappacgs2gu * (2.13e39 * (nethcgs / rhocgs) / te5 * ia_by_b_num) * rho;
-        if (bridge) kapparadnumsyn *= (te / tc_n) / (1.0 + te / tc_n);
+        double ia_by_b_num = kmath::div(bmagcgs, zeta_a_denom_num);
+        kapparadnumsyn = c.kappacgs2gu * (kmath::div(2.13e39 * (kmath::div(nethcgs, rhocgs)), te5) * ia_by_b_num) * rho;
+        if (bridge) kapparadnumsyn *= kmath::div((kmath::div(te, tc_n)), (1.0 + kmath::div(te, tc_n)));
       }
       double bmb = (bmagcgs > 0.0) ? kmath::pow(bmagcgs, -0.463) : 0.0;
       double ia_by_b_ross_rad =
-          0.13 * kmath::pow(bmagcgs, 0.69) / (kmath::pow(zbr, 1.69) * kmath::exp(1.6 * kmath::pow(zbr, 0.463) * bmb));
-      kapparadsynross = c.kappacgs2gu * (2.13e39 * (nethcgs / rhocgs) / te5 * ia_by_b_ross_rad) * rho;
+          kmath::div(0.13 * kmath::pow(bmagcgs, 0.69), (kmath::pow(zbr, 1.69) * kmath::exp(1.6 * kmath::pow(zbr, 0.463) * bmb)));
+      kapparadsynross = c.kappacgs2gu * (kmath::div(2.13e39 * (kmath::div(nethcgs, rhocgs)), te5) * ia_by_b_ross_rad) * rho;
       if (want_full) {
-        double zbg = c.k_boltz_cgs * te / c.h_cgs / nu_mbsyn;
+        double zbg = kmath::div(kmath::div(c.k_boltz_cgs * te, c.h_cgs), nu_mbsyn);
         double ia_by_b_ross_gas =
-            0.13 * kmath::pow(bmagcgs, 0.69) / (kmath::pow(zbg, 1.69) * kmath::exp(1.6 * kmath::pow(zbg, 0.463) * bmb));
-        kappagassynross = c.kappacgs2gu * (2.13e39 * (nethcgs / rhocgs) / te5 * ia_by_b_ross_gas) * rho;
+            kmath::div(0.13 * kmath::pow(bmagcgs, 0.69), (kmath::pow(zbg, 1.69) * kmath::exp(1.6 * kmath::pow(zbg, 0.463) * bmb)));
+        kappagassynross = c.kappacgs2gu * (kmath::div(2.13e39 * (kmath::div(nethcgs, rhocgs)), te5) * ia_by_b_ross_gas) * rho;
       }
     }
     if (bridge)
-      kappagassyn += c.kappacgs2gu * (2.35869e-21 * (nethcgs / rhocgs) * (bmagcgs * bmagcgs) / (te * te * te)) * rho;
+      kappagassyn += c.kappacgs2gu * (kmath::div(2.35869e-21 * (kmath::div(nethcgs, rhocgs)) * (bmagcgs * bmagcgs), (te * te * te))) * rho;
     if (!bridge) {
       double terel = te * c.k_over_mecsq;
-      double terelfactor = (terel * terel) / (1.0 + terel * terel);
+      double terelfactor = kmath::div((terel * terel), (1.0 + terel * terel));
       kappagassyn *= terelfactor;
       if (want_rad) {
         kapparadsyn *= terelfactor;
@@ -199,7 +199,7 @@ KC_HD double kappaes_puffy(const Consts& c, const Channels& ch, double rho, doub
   double opac_correction = 1.0;
   if (ch.kleinnishina) {
     double tkn = trad;
-    opac_correction = 1.0 / (1.0 + kmath::pow(tkn / 4.5e8, 0.86));
+    opac_correction = kmath::div(1.0, (1.0 + kmath::pow(kmath::div(tkn, 4.5e8), 0.86)));
   }
   return ((0.2 * (1.0 + c.hfrac)) * opac_correction) * c.kappa_cgs2gu_fac * rho;
 }
@@ -277,7 +277,7 @@ KC_HD void lorentz_from_pair(const double ucon[4], const double ucov[4], const d
     for (int j = 0; j < 4; ++j) {
       double omsum = 0.0;
       for (int k = 0; k < 4; ++k) omsum += om[i][k] * om[k][j];
-      l[i][j] = kron(i, j) + 1.0 / (1.0 + gam) * omsum + om[i][j];
+      l[i][j] = kron(i, j) + kmath::div(1.0, (1.0 + gam)) * omsum + om[i][j];
     }
 }
 KC_HD void normal_obs_concov(const Geom& g, double con[4], double cov[4]) {
@@ -307,16 +307,16 @@ KC_HDM void boost2_lab2ff(const double a1[4], double v1, double v2, double v3, c
   double l[4][4];
   lorentz_lab2ff(v1, v2, v3, g, l);
   transform_vec(a1, l, a2);
-  double alpha = kmath::sqrt(-1.0 / g.GG[0][0]);
+  double alpha = kmath::sqrt(kmath::div(-1.0, g.GG[0][0]));
   for (int i = 0; i < 4; ++i) a2[i] *= alpha;
 }
 // A2 = L_ff2lab (A1 / alpha) (frames.zig:108, C boost2_ff2lab)
 KC_HDM void boost2_ff2lab(const double a1[4], double v1, double v2, double v3, const Geom& g, double a2[4]) {
   double l[4][4];
   lorentz_ff2lab(v1, v2, v3, g, l);
-  double alpha = kmath::sqrt(-1.0 / g.GG[0][0]);
+  double alpha = kmath::sqrt(kmath::div(-1.0, g.GG[0][0]));
   double at[4];
-  for (int i = 0; i < 4; ++i) at[i] = a1[i] / alpha;
+  for (int i = 0; i < 4; ++i) at[i] = kmath::div(a1[i], alpha);
   transform_vec(at, l, a2);
 }
 // T2 = L L T1, no alpha (frames.zig:147, C boost22_ff2lab)
@@ -329,8 +329,8 @@ KC_HDM void boost22_ff2lab(const double t1[4][4], double v1, double v2, double v
 // ---- four-force (koral/physics/radforce.zig:370-494) ------------------------
 KC_HD double compton_gi_coeff(const Consts& c, const RadState& st) {
   double thetae = c.kb_over_me * st.te;
-  return st.kappaes * st.ehat * ((4.0 * c.kb_over_me) * (st.trad - st.te)) *
-         (1.0 + 3.683 * thetae + 4.0 * thetae * thetae) / (1.0 + 4.0 * thetae);
+  return kmath::div(st.kappaes * st.ehat * ((4.0 * c.kb_over_me) * (st.trad - st.te)) *
+         (1.0 + 3.683 * thetae + 4.0 * thetae * thetae), (1.0 + 4.0 * thetae));
 }
 // C calc_all_Gi_with_state thermal part (radforce.zig:432). full=false leaves
 // ff[1..3] zero and skips the boost (the solver path).

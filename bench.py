@@ -61,6 +61,23 @@ def pass_bytes(name, ndim):
     return PASS_BYTES_PER_CELL.get(name)
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's device time (every rank calls this, in the same order)."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(cells_per_rank, steps, world, ms_max):
+    """Whole-job zone-cycles/s of `world` replicas: all ranks' cells x steps over
+    the slowest rank's time."""
+    return cells_per_rank * steps * world / (ms_max / 1e3)
+
+
 def load_engine():
     spec = importlib.util.spec_from_file_location("koralcuda", os.path.join(ROOT, "koral-zig_b200", "koralcuda.py"))
     mod = importlib.util.module_from_spec(spec)
@@ -431,12 +448,8 @@ def main():
     launches = sim.launch_count() - n0
     passes = sim.pass_times()
     sim.set_pass_timing(False)
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = ncell * args.steps * world / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = job_rate(ncell, args.steps, world, ms_max)
 
     # ---- end to end through the C ABI with host buffers (e2e) ---------------------
     # Each step: pinned host p, u, flags -> device, Sim.step, device -> host; the
@@ -464,13 +477,9 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ems = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
+    ems = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     e2e_bytes = hp.nbytes + hu.nbytes + hf.nbytes
-    e2e = {"value": ncell * ke * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": e2e_bytes,
+    e2e = {"value": job_rate(ncell, ke, world, ems), "unit": UNIT, "h2d_bytes_per_step": e2e_bytes,
            "d2h_bytes_per_step": e2e_bytes, "steps": ke}
 
     # ---- roofline of the dominant pass ---------------------------------------------

@@ -467,10 +467,11 @@ KC_HD void implicit_rung(int ir, int startwith, int& p, int& e, int& fr) {
   }
 }
 
-// C solve_implicit_lab (implicit.zig:927) — the rung ladder; on success pp
-// and uu are overwritten, on failure untouched.
-KC_HDN ImplicitResult solve_implicit_lab(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
-                                         const RadParams& rad, const OpacParams& op, const ImplicitParams& ip) {
+// the rung ladder of solve_implicit_lab (implicit.zig:963) from a prepared
+// state: on success pp and uu are overwritten, on failure untouched
+KC_HDN ImplicitResult implicit_ladder(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
+                                      const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
+                                      const ImplicitPre& pre) {
   ImplicitResult res;
   res.ok = 0;
   res.rung = -1;
@@ -478,8 +479,6 @@ KC_HDN ImplicitResult solve_implicit_lab(double uu[NV], double pp[NV], const Geo
   res.whichprim = PRIM_RAD;
   res.whicheq = EQ_ENERGY;
   res.whichframe = FRAME_LAB;
-  ImplicitPre pre;
-  implicit_prepare(pp, g, dt, gam, op, ip, pre);
   for (int level = 0; level <= ip.opdamp_maxlevels; ++level) {
     OpacParams opl = op;
     double od = 1.0;
@@ -504,6 +503,73 @@ KC_HDN ImplicitResult solve_implicit_lab(double uu[NV], double pp[NV], const Geo
     }
   }
   return res;
+}
+
+// C solve_implicit_lab (implicit.zig:927) — the rung ladder; on success pp
+// and uu are overwritten, on failure untouched.
+KC_HDN ImplicitResult solve_implicit_lab(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
+                                         const RadParams& rad, const OpacParams& op, const ImplicitParams& ip) {
+  ImplicitPre pre;
+  implicit_prepare(pp, g, dt, gam, op, ip, pre);
+  return implicit_ladder(uu, pp, g, dt, gam, rad, op, ip, pre);
+}
+
+// The first-rung residual the Newton core evaluates at a start state before
+// its first Jacobian (the opening of solve_4dprim_core: constraints, state
+// fill, residual) and the constrained start in pp; +inf when the constraints
+// reject the start.
+KC_HD double implicit_start_residual(const double uu00[NV], const RadState& state00, const double start[NV],
+                                     const Geom& g, double dt, double gam, const RadParams& rad,
+                                     const OpacParams& op, const ImplicitParams& ip, int whichprim, double pp[NV]) {
+  double uu[NV], f[4];
+  for (int i = 0; i < NV; ++i) {
+    uu[i] = uu00[i];
+    pp[i] = start[i];
+  }
+  if (apply_constraints(pp, uu, uu00, g, gam, rad, ip, whichprim) < -1) return 1.0e300;
+  RadState st;
+  fill_rad_state(pp, g, gam, op, false, st);
+  if (ip.lag_opac) lag_opac(st, state00);
+  return implicit_residual(uu, pp, st, uu00, state00, dt, g, op, whichprim, EQ_ENERGY, FRAME_LAB, f);
+}
+
+// The same ladder started from a learned state in place of the bisection warm
+// start (the learned-guess form; it has no counterpart in the reference).
+// The start fluid is decided as solve_implicit_lab decides it. A cell the
+// pre-solve state already satisfies (first-rung residual below conv, the
+// core's first exit) is finished there, as the core would finish it, so a
+// prediction error never costs such a cell an iteration; the others run the
+// ladder from whichever of the pre-solve and the learned state has the
+// smaller first-rung residual (starting every such cell from the learned
+// state measured slower: the prediction is worse than the pre-solve state for
+// a part of them).
+KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
+                                              const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
+                                              const double guess[NV]) {
+  ImplicitPre pre;
+  p2u(pp, pre.uu00, g, gam);
+  double ehat = -calc_ff_rtt(pp, g, nullptr);
+  fill_rad_state(pp, g, gam, op, true, pre.state00);
+  pre.startwith = (ehat < ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
+  double pc[NV];
+  double e0 = implicit_start_residual(pre.uu00, pre.state00, pp, g, dt, gam, rad, op, ip, pre.startwith, pc);
+  if (e0 < ip.conv) {
+    // the core's first exit on rung 0 (lab frame, energy equation)
+    ImplicitResult res;
+    for (int i = 0; i < NV; ++i) pp[i] = pc[i];
+    p2u(pc, uu, g, gam);
+    res.ok = 1;
+    res.rung = 0;
+    res.iters = 1;
+    res.whichprim = pre.startwith;
+    res.whicheq = EQ_ENERGY;
+    res.whichframe = FRAME_LAB;
+    return res;
+  }
+  double e1 = implicit_start_residual(pre.uu00, pre.state00, guess, g, dt, gam, rad, op, ip, pre.startwith, pc);
+  bool learned = e1 < e0;
+  for (int i = 0; i < NV; ++i) pre.pp0[i] = learned ? guess[i] : pp[i];
+  return implicit_ladder(uu, pp, g, dt, gam, rad, op, ip, pre);
 }
 
 }  // namespace kp

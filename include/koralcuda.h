@@ -218,7 +218,52 @@ int kc_get_launch_count(kc_handle* h, int64_t* n);
 /* Engine forms (no reference counterpart) */
 int kc_set_precision(kc_handle* h, int32_t mode);
 int kc_set_implicit_mode(kc_handle* h, int32_t mode);
+
+/* The learned initial guess of the implicit solve (no reference counterpart).
+ * A 16 -> 64 -> 64 -> 4 ReLU network predicts, from a cell's pre-solve
+ * primitives, the four Newton unknowns of the start fluid; the FP64 Newton
+ * ladder then starts from that state instead of the bisection warm start of
+ * koral/solve/implicit.zig:944, and the plain solve runs when the seeded ladder
+ * fails. Weights are one FP32 blob of KC_MLP_NWEIGHTS floats: input mean[16],
+ * input std[16], output mean[4], output std[4], W1[64][16], b1[64],
+ * W2[64][64], b2[64], W3[4][64], b3[4] (row-major [out][in]). Inference runs
+ * on the tensor cores with BF16 weights and activations and FP32
+ * accumulation. Features (before standardisation): log10 rho, log10 u_int,
+ * asinh(1e3 v^i), +1/-1 for a gas/radiation start, asinh(1e12 B^i),
+ * log10 E_rad, asinh(1e3 F^i), log10 dt, log10 sqrt(-g), alpha. Targets:
+ * asinh(ln(e_sol / e_0) / 1e-7) for the start fluid's energy density and
+ * asinh((v_sol - v_0) / max(1e-6, |v_0|) / 1e-9) for its velocities (the
+ * changes in the units of the Newton convergence test, compressed).
+ * kc_set_guess(KC_GUESS_MLP) installs the weights for the handle's steps
+ * (KC_GUESS_PLAIN returns to the reference path). The learned guess and the
+ * harvest run the per-cell implicit form. */
+enum { KC_MLP_IN = 16, KC_MLP_HIDDEN = 64, KC_MLP_OUT = 4, KC_MLP_NWEIGHTS = 5548 };
 int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweights);
+/* Training pairs from the handle's own steps: from the next implicit pass on,
+ * each cell whose solve converged on the first rung stores its features and
+ * targets, up to `capacity` pairs (0 stops the harvest); kc_get_harvest copies
+ * the pairs collected so far out and sets *n. */
+int kc_harvest_implicit(kc_handle* h, int64_t capacity);
+int kc_get_harvest(kc_handle* h, float* features, float* targets, int64_t capacity, int64_t* n);
+/* seeded ladders that failed and fell back to the plain solve, since the
+ * guess was first installed */
+int64_t kc_guess_fallbacks(kc_handle* h);
+/* Trains the network on the GPU (FP32 forward/backward kernels with the
+ * weights rounded to BF16 in the forward pass, Adam): normalisation from the
+ * pairs (feature deviations floored at 0.01; standardised features clipped to
+ * +-8, as the guess clips its inputs and outputs), He-uniform start from
+ * `seed`, `steps` minibatches of `batch` pairs.
+ * weights_out gets the blob; loss_curve (may be NULL) the mean squared error
+ * of each step's minibatch in standardised units. Host arrays. */
+int kc_mlp_train(const float* features, const float* targets, int64_t n, int32_t steps, int32_t batch, float lr,
+                 uint64_t seed, float* weights_out, float* loss_curve);
+/* The tensor-core forward pass on standardised features (n x 16) into
+ * standardised outputs (n x 4); and the training kernels' loss (mean squared
+ * error) and its gradient with respect to the blob (entries before W1 are
+ * zero) over all n pairs. Host arrays. */
+int kc_mlp_forward(const float* weights, int64_t n, const float* features_std, float* out_std);
+int kc_mlp_grad(const float* weights, int64_t n, const float* features_std, const float* targets_std, float* grad,
+                float* loss);
 
 /* Batched per-cell entry points over n independent cells (the C4 implicit
  * microbench and the parity harnesses). geom23 is the reference's golden

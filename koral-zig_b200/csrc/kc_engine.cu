@@ -4,6 +4,8 @@
 // fixed sequence of kernel launches on that stream with no host round trip
 // until the step's scalars are read back at its end.
 #include <math.h>
+
+#include <cmath>
 #include <stdio.h>
 #include <string.h>
 
@@ -58,6 +60,15 @@ struct kc_handle {
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
   int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
+  // the learned initial guess (KC_GUESS_MLP): FP32 blob, BF16 weight copies,
+  // the per-cell seeded starts, and the training-pair harvest buffers
+  int guess_mode = KC_GUESS_PLAIN;
+  float* mlp_blob = nullptr;
+  __nv_bfloat16 *mlp_w1 = nullptr, *mlp_w2 = nullptr, *mlp_w3 = nullptr;
+  double* guess = nullptr;
+  unsigned long long* imp_ctr = nullptr;  // [0] seeded-ladder fallbacks, [1] harvested pairs
+  float *hx = nullptr, *ht = nullptr;
+  long hcap = 0;
   // scalar diagnostics: fold outputs and counts, and the BL geometry of the
   // luminosity shell (built on the host at first use for that shell)
   double* diag = nullptr;
@@ -350,7 +361,9 @@ void launch_implicit(kc_handle* h, double dtin) {
   a.ip = h->sp.ip;
   a.polar_nc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
   PassScope ps(h, KC_PASS_IMPLICIT);
-  if (h->opt.implicit_mode == KC_IMPLICIT_COMPACTING) {
+  // the learned guess and the harvest run in the per-cell form
+  bool extra = h->guess_mode == KC_GUESS_MLP || h->hcap > 0;
+  if (h->opt.implicit_mode == KC_IMPLICIT_COMPACTING && !extra) {
     long nwork = (long)gr.nx * (gr.ny - 2L * a.polar_nc) * gr.nz;
     if (h->impl_blocks == 0) {
       int dev = 0, nsm = 0, per_sm = 0;
@@ -366,8 +379,26 @@ void launch_implicit(kc_handle* h, double dtin) {
     if (blocks > 0) k_implicit_persistent<<<blocks, TPB, 0, h->stream>>>(h->ds, h->dsc, a, nwork);
     return;
   }
+  long ndom = (long)gr.nx * gr.ny * gr.nz;
+  ImplExtra x = {nullptr, nullptr, nullptr, nullptr, 0, nullptr};
+  if (h->imp_ctr) {
+    x.n_fallback = h->imp_ctr;
+    if (h->hcap > 0) {
+      x.hx = h->hx;
+      x.ht = h->ht;
+      x.hcount = h->imp_ctr + 1;
+      x.hcap = h->hcap;
+    }
+  }
+  if (h->guess_mode == KC_GUESS_MLP) {
+    MlpDev m = {h->mlp_w1, h->mlp_w2, h->mlp_w3, h->mlp_blob};
+    ++h->n_launch;
+    k_mlp_guess<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, m, a, h->guess);
+    x.guess = h->guess;
+  }
   ++h->n_launch;
-  k_implicit<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
+  if (extra) k_implicit<true><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  else k_implicit<false><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
 }
 
 void launch_wavespeeds(kc_handle* h) {
@@ -1014,12 +1045,79 @@ int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
   h->opt.implicit_mode = mode;
   return KC_OK;
 }
+static int ensure_imp_ctr(kc_handle* h) {
+  int st = 0;
+  if (!h->imp_ctr) h->imp_ctr = dalloc<unsigned long long>(h, 2, st);
+  return st;
+}
 int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweights) {
-  (void)weights;
-  (void)nweights;
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (mode != KC_GUESS_PLAIN) return fail(h, KC_ERR_INVALID_CONFIG, "learned guess not built");
+  if (mode == KC_GUESS_PLAIN) {
+    h->guess_mode = KC_GUESS_PLAIN;
+    return KC_OK;
+  }
+  if (mode != KC_GUESS_MLP) return fail(h, KC_ERR_INVALID_CONFIG, "unknown guess mode");
+  if (!weights || nweights != KC_MLP_NWEIGHTS)
+    return fail(h, KC_ERR_INVALID_CONFIG, "learned guess needs KC_MLP_NWEIGHTS floats");
+  for (int64_t i = 0; i < nweights; ++i)
+    if (!std::isfinite(weights[i])) return fail(h, KC_ERR_INVALID_CONFIG, "non-finite guess weight");
+  for (int k = 0; k < MLP_IN; ++k)
+    if (!(weights[MLP_OFF_ISTD + k] > 0.0f)) return fail(h, KC_ERR_INVALID_CONFIG, "guess input std must be > 0");
+  int st = ensure_imp_ctr(h);
+  const DGrid& gr = h->gr;
+  long ndom = (long)gr.nx * gr.ny * gr.nz;
+  if (!h->mlp_blob) {
+    h->mlp_blob = dalloc<float>(h, MLP_NW, st);
+    h->mlp_w1 = dalloc<__nv_bfloat16>(h, MLP_H * MLP_IN, st);
+    h->mlp_w2 = dalloc<__nv_bfloat16>(h, MLP_H * MLP_H, st);
+    h->mlp_w3 = dalloc<__nv_bfloat16>(h, 8 * MLP_H, st);
+    h->guess = dalloc<double>(h, (size_t)NV * ndom, st);
+  }
+  if (st) return st;
+  int e = cuda_check(h, cudaMemcpyAsync(h->mlp_blob, weights, MLP_NW * 4, cudaMemcpyHostToDevice, h->stream),
+                     "guess weights");
+  if (e) return e;
+  k_mlp_pack<<<(MLP_H * MLP_H + 127) / 128, 128, 0, h->stream>>>(h->mlp_blob, h->mlp_w1, h->mlp_w2, h->mlp_w3);
+  e = cuda_check(h, cudaStreamSynchronize(h->stream), "guess pack");
+  if (e) return e;
+  h->guess_mode = KC_GUESS_MLP;
   return KC_OK;
+}
+int kc_harvest_implicit(kc_handle* h, int64_t capacity) {
+  if (!h || capacity < 0) return KC_ERR_INVALID_CONFIG;
+  int st = ensure_imp_ctr(h);
+  if (st) return st;
+  if (capacity > h->hcap) {
+    h->hx = dalloc<float>(h, (size_t)capacity * MLP_IN, st);
+    h->ht = dalloc<float>(h, (size_t)capacity * MLP_OUT, st);
+    if (st) return st;
+  }
+  h->hcap = capacity;
+  return cuda_check(h, cudaMemsetAsync(h->imp_ctr + 1, 0, 8, h->stream), "harvest reset");
+}
+int kc_get_harvest(kc_handle* h, float* features, float* targets, int64_t capacity, int64_t* n_out) {
+  if (!h || !n_out || capacity < 0) return KC_ERR_INVALID_CONFIG;
+  *n_out = 0;
+  if (!h->imp_ctr || h->hcap == 0) return KC_OK;
+  unsigned long long cnt = 0;
+  int e = cuda_check(h, cudaMemcpyAsync(&cnt, h->imp_ctr + 1, 8, cudaMemcpyDeviceToHost, h->stream), "harvest count");
+  if (!e) e = cuda_check(h, cudaStreamSynchronize(h->stream), "harvest count");
+  if (e) return e;
+  long n = (long)cnt < h->hcap ? (long)cnt : h->hcap;
+  if (n > capacity) n = capacity;
+  if (n > 0 && features)
+    e = cuda_check(h, cudaMemcpy(features, h->hx, (size_t)n * MLP_IN * 4, cudaMemcpyDeviceToHost), "harvest x");
+  if (!e && n > 0 && targets)
+    e = cuda_check(h, cudaMemcpy(targets, h->ht, (size_t)n * MLP_OUT * 4, cudaMemcpyDeviceToHost), "harvest t");
+  if (e) return e;
+  *n_out = n;
+  return KC_OK;
+}
+int64_t kc_guess_fallbacks(kc_handle* h) {
+  if (!h || !h->imp_ctr) return 0;
+  unsigned long long v = 0;
+  cudaMemcpy(&v, h->imp_ctr, 8, cudaMemcpyDeviceToHost);
+  return (int64_t)v;
 }
 // The PUFFY init sequence (puffy.zig:873 initAllWith, then initTimestepGuess as
 // problems/puffy/main.zig:304 does). The limotorus profile and the per-cell
@@ -1471,5 +1569,149 @@ extern "C" int kc_implicit_batch_noalloc(const kc_options* opt, int64_t n, const
   if (cudaMemcpy(pp, dp, (size_t)n * NV * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
       cudaMemcpy(res, dr, (size_t)n * 6 * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
     return KC_ERR_CUDA;
+  return KC_OK;
+}
+
+// ---- the learned-guess network: training, forward and gradient entry points --
+namespace {
+static_assert(MLP_NW == KC_MLP_NWEIGHTS, "weight blob size");
+// minibatch indices of one training step: splitmix64 of (seed, step, slot)
+__global__ void k_mlp_sample(long* idx, long nb, long n, uint64_t seed, long step) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(step * nb + i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z ^= z >> 31;
+  idx[i] = (long)(z % (uint64_t)n);
+}
+const int MLP_ACT = MLP_IN + 4 * MLP_H + MLP_OUT;  // per-sample training record (floats)
+int mlp_device() {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return KC_ERR_NO_DEVICE;
+  return KC_OK;
+}
+}  // namespace
+
+extern "C" int kc_mlp_forward(const float* weights, int64_t n, const float* features_std, float* out_std) {
+  int st = mlp_device();
+  if (st) return st;
+  if (!weights || n < 0 || (n > 0 && (!features_std || !out_std))) return KC_ERR_INVALID_CONFIG;
+  if (n == 0) return KC_OK;
+  DevBuf db, dw1, dw2, dw3, dx, dy;
+  if (cudaMalloc(&db.p, MLP_NW * 4) || cudaMalloc(&dw1.p, MLP_H * MLP_IN * 2) || cudaMalloc(&dw2.p, MLP_H * MLP_H * 2) ||
+      cudaMalloc(&dw3.p, 8 * MLP_H * 2) || cudaMalloc(&dx.p, n * MLP_IN * 4) || cudaMalloc(&dy.p, n * MLP_OUT * 4))
+    return KC_ERR_OOM;
+  cudaMemcpy(db.p, weights, MLP_NW * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dx.p, features_std, n * MLP_IN * 4, cudaMemcpyHostToDevice);
+  k_mlp_pack<<<(MLP_H * MLP_H + 127) / 128, 128>>>((const float*)db.p, (__nv_bfloat16*)dw1.p, (__nv_bfloat16*)dw2.p,
+                                                   (__nv_bfloat16*)dw3.p);
+  MlpDev m = {(const __nv_bfloat16*)dw1.p, (const __nv_bfloat16*)dw2.p, (const __nv_bfloat16*)dw3.p,
+              (const float*)db.p};
+  k_mlp_forward<<<nblk(n), TPB>>>(m, n, (const float*)dx.p, (float*)dy.p);
+  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  cudaMemcpy(out_std, dy.p, n * MLP_OUT * 4, cudaMemcpyDeviceToHost);
+  return KC_OK;
+}
+
+extern "C" int kc_mlp_grad(const float* weights, int64_t n, const float* features_std, const float* targets_std,
+                           float* grad, float* loss) {
+  int st = mlp_device();
+  if (st) return st;
+  if (!weights || !grad || !loss || n <= 0 || !features_std || !targets_std) return KC_ERR_INVALID_CONFIG;
+  DevBuf db, dx, dt, da, dg, dl;
+  if (cudaMalloc(&db.p, MLP_NW * 4) || cudaMalloc(&dx.p, n * MLP_IN * 4) || cudaMalloc(&dt.p, n * MLP_OUT * 4) ||
+      cudaMalloc(&da.p, n * MLP_ACT * 4) || cudaMalloc(&dg.p, MLP_NW * 4) || cudaMalloc(&dl.p, 4))
+    return KC_ERR_OOM;
+  cudaMemcpy(db.p, weights, MLP_NW * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dx.p, features_std, n * MLP_IN * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dt.p, targets_std, n * MLP_OUT * 4, cudaMemcpyHostToDevice);
+  cudaMemset(dg.p, 0, MLP_NW * 4);
+  cudaMemset(dl.p, 0, 4);
+  k_mlp_train_fwd<<<nblk(n), TPB>>>((const float*)db.p, (const float*)dx.p, (const float*)dt.p, nullptr, n,
+                                    (float*)da.p, (float*)dl.p);
+  k_mlp_train_grad<<<(MLP_NW + 127) / 128, 128>>>((const float*)da.p, n, (float*)dg.p);
+  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  cudaMemcpy(grad, dg.p, MLP_NW * 4, cudaMemcpyDeviceToHost);
+  float l = 0.0f;
+  cudaMemcpy(&l, dl.p, 4, cudaMemcpyDeviceToHost);
+  *loss = l / (float)(n * MLP_OUT);
+  return KC_OK;
+}
+
+// Training: the normalisation (per-column mean and standard deviation) is
+// taken from the pairs on the host, the feature deviations floored at
+// MLP_FEATURE_STD_MIN and the standardised features clipped to
+// +-MLP_STD_CLIP as inference clips them; the weights start He-uniform
+// from `seed` (biases zero); each step draws `batch` pairs, runs the forward
+// and backward kernels and an Adam update with learning rate `lr`.
+extern "C" int kc_mlp_train(const float* features, const float* targets, int64_t n, int32_t steps, int32_t batch,
+                            float lr, uint64_t seed, float* weights_out, float* loss_curve) {
+  int st = mlp_device();
+  if (st) return st;
+  if (!features || !targets || !weights_out || n <= 0 || steps < 0 || batch <= 0 || !(lr > 0.0f))
+    return KC_ERR_INVALID_CONFIG;
+  std::vector<float> w(MLP_NW, 0.0f), xs((size_t)n * MLP_IN), ts((size_t)n * MLP_OUT);
+  auto standardise = [&](const float* src, int cols, int off_mean, int off_std, double floor, double clip,
+                         float* dst) {
+    for (int k = 0; k < cols; ++k) {
+      double s = 0.0, q = 0.0;
+      for (int64_t i = 0; i < n; ++i) s += src[i * cols + k];
+      double mu = s / (double)n;
+      for (int64_t i = 0; i < n; ++i) q += (src[i * cols + k] - mu) * (src[i * cols + k] - mu);
+      double sd = std::sqrt(q / (double)n);
+      if (!(sd > floor)) sd = floor;
+      w[off_mean + k] = (float)mu;
+      w[off_std + k] = (float)sd;
+      for (int64_t i = 0; i < n; ++i) {
+        double z = ((double)src[i * cols + k] - (double)w[off_mean + k]) / (double)w[off_std + k];
+        dst[i * cols + k] = (float)(z > clip ? clip : (z < -clip ? -clip : z));
+      }
+    }
+  };
+  standardise(features, MLP_IN, MLP_OFF_IMEAN, MLP_OFF_ISTD, MLP_FEATURE_STD_MIN, MLP_STD_CLIP, xs.data());
+  standardise(targets, MLP_OUT, MLP_OFF_OMEAN, MLP_OFF_OSTD, 1.0e-30, 1.0e30, ts.data());
+  for (float v : xs)
+    if (!std::isfinite(v)) return KC_ERR_INVALID_CONFIG;
+  for (float v : ts)
+    if (!std::isfinite(v)) return KC_ERR_INVALID_CONFIG;
+  XorShift rng{seed ? seed : 0x2545F4914F6CDD1DULL};
+  auto he = [&](int off, int rows, int cols) {
+    double a = std::sqrt(6.0 / cols);
+    for (int i = 0; i < rows * cols; ++i) w[off + i] = (float)(a * rng.pm());
+  };
+  he(MLP_OFF_W1, MLP_H, MLP_IN);
+  he(MLP_OFF_W2, MLP_H, MLP_H);
+  he(MLP_OFF_W3, MLP_OUT, MLP_H);
+  long nb = batch < n ? batch : n;
+  DevBuf db, dg, dm1, dm2, dx, dt, di, da, dl;
+  if (cudaMalloc(&db.p, MLP_NW * 4) || cudaMalloc(&dg.p, MLP_NW * 4) || cudaMalloc(&dm1.p, MLP_NW * 4) ||
+      cudaMalloc(&dm2.p, MLP_NW * 4) || cudaMalloc(&dx.p, n * MLP_IN * 4) || cudaMalloc(&dt.p, n * MLP_OUT * 4) ||
+      cudaMalloc(&di.p, nb * 8) || cudaMalloc(&da.p, nb * MLP_ACT * 4) || cudaMalloc(&dl.p, (steps + 1) * 4))
+    return KC_ERR_OOM;
+  cudaMemcpy(db.p, w.data(), MLP_NW * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dx.p, xs.data(), n * MLP_IN * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dt.p, ts.data(), n * MLP_OUT * 4, cudaMemcpyHostToDevice);
+  cudaMemset(dm1.p, 0, MLP_NW * 4);
+  cudaMemset(dm2.p, 0, MLP_NW * 4);
+  cudaMemset(dl.p, 0, (steps + 1) * 4);
+  double b1 = 1.0, b2 = 1.0;
+  for (int s = 0; s < steps; ++s) {
+    b1 *= 0.9;
+    b2 *= 0.999;
+    k_mlp_sample<<<nblk(nb), TPB>>>((long*)di.p, nb, n, seed, s);
+    k_mlp_train_fwd<<<nblk(nb), TPB>>>((const float*)db.p, (const float*)dx.p, (const float*)dt.p,
+                                       (const long*)di.p, nb, (float*)da.p, (float*)dl.p + s);
+    k_mlp_train_grad<<<(MLP_NW + 127) / 128, 128>>>((const float*)da.p, nb, (float*)dg.p);
+    k_mlp_adam<<<(MLP_NW + 127) / 128, 128>>>((float*)db.p, (const float*)dg.p, (float*)dm1.p, (float*)dm2.p, lr,
+                                              (float)(1.0 - b1), (float)(1.0 - b2));
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
+  cudaMemcpy(weights_out, db.p, MLP_NW * 4, cudaMemcpyDeviceToHost);
+  if (loss_curve && steps > 0) {
+    std::vector<float> l(steps);
+    cudaMemcpy(l.data(), dl.p, steps * 4, cudaMemcpyDeviceToHost);
+    for (int s = 0; s < steps; ++s) loss_curve[s] = l[s] / (float)(nb * MLP_OUT);
+  }
   return KC_OK;
 }

@@ -7,6 +7,7 @@
 #include "kc_dev.cuh"
 #include "kc_implicit_sm.cuh"
 #include "kc_mixed.cuh"
+#include "kc_mlp.cuh"
 
 namespace kc {
 
@@ -843,7 +844,19 @@ struct ImplArgs {
   ImplicitParams ip;
   int polar_nc;
 };
-__global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, ImplArgs a) {
+// the learned-guess form and the training-pair harvest of the implicit pass
+struct ImplExtra {
+  const double* guess;  // [NV][nx ny nz] seeded starting states, or null (plain form)
+  float* hx;            // harvest: features [cap][16], targets [cap][4], or null
+  float* ht;
+  unsigned long long* hcount;
+  long hcap;
+  unsigned long long* n_fallback;  // seeded ladders that failed and fell back to the plain path
+};
+// EXTRA = false is the reference path alone (the guess and harvest code is not
+// compiled into it, so its registers and code size are those of the plain solve)
+template <bool EXTRA>
+__global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, ImplArgs a, ImplExtra x) {
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
   if (!range_cell(r, ix, iy, iz)) return;
@@ -854,7 +867,31 @@ __global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, Im
   load_cell(s.p, nc, c, pp);
   Geom g;
   geom_cell(s, ix, iy, iz, g);
-  ImplicitResult res = solve_implicit_lab(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip);
+  double pp00[NV];
+  if (EXTRA)
+    for (int i = 0; i < NV; ++i) pp00[i] = pp[i];
+  ImplicitResult res;
+  if (EXTRA && x.guess) {
+    long nd = (long)s.gr.nx * s.gr.ny * s.gr.nz, td = ix + s.gr.nx * (iy + s.gr.ny * iz);
+    double g0[NV];
+    for (int i = 0; i < NV; ++i) g0[i] = x.guess[i * nd + td];
+    res = solve_implicit_lab_from(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip, g0);
+    if (!res.ok) {
+      atomicAdd(x.n_fallback, 1ULL);
+      res = solve_implicit_lab(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip);
+    }
+  } else {
+    res = solve_implicit_lab(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip);
+  }
+  if (EXTRA && x.hx && res.ok && res.rung == 0) {
+    unsigned long long k = atomicAdd(x.hcount, 1ULL);
+    if ((long)k < x.hcap) {
+      double ehat = -calc_ff_rtt(pp00, g, nullptr);
+      int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
+      mlp_features_raw(pp00, a.dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
+      mlp_targets_raw(pp00, pp, sw, x.ht + k * MLP_OUT);
+    }
+  }
   if (res.ok) {
     store_cell(s.u, nc, c, uu);
     store_cell(s.p, nc, c, pp);
@@ -865,6 +902,55 @@ __global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, Im
     s.flags[5 * nc + c] = -1;
     atomicAdd(&sc->n_fail, 1ULL);
   }
+}
+
+// The learned guess per domain cell: features of the pre-solve state,
+// standardised, through the tensor-core network (one warp per 32 cells), and
+// the seeded starting state written to guess [NV][nx ny nz].
+__global__ void __launch_bounds__(128) k_mlp_guess(DevState s, MlpDev m, ImplArgs a, double* guess) {
+  __shared__ float xs[4][32 * MLP_IN];
+  __shared__ float ys[4][32 * MLP_OUT];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long nx = s.gr.nx, ny = s.gr.ny, nd = nx * ny * s.gr.nz;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool valid = t < nd;
+  double pp[NV];
+  int sw = PRIM_MHD;
+  float f[MLP_IN];
+  for (int k = 0; k < MLP_IN; ++k) f[k] = 0.0f;
+  if (valid) {
+    long ix = t % nx, iy = (t / nx) % ny, iz = t / (nx * ny);
+    long c = cidx(s.gr, ix, iy, iz);
+    load_cell(s.p, s.gr.nc, c, pp);
+    Geom g;
+    geom_cell(s, ix, iy, iz, g);
+    double ehat = -calc_ff_rtt(pp, g, nullptr);
+    sw = (ehat < a.ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
+    mlp_features_raw(pp, a.dt, g.gdet, g.alpha, sw, f);
+    for (int k = 0; k < MLP_IN; ++k) f[k] = mlp_clip((f[k] - m.blob[MLP_OFF_IMEAN + k]) / m.blob[MLP_OFF_ISTD + k]);
+  }
+  for (int k = 0; k < MLP_IN; ++k) xs[warp][lane * MLP_IN + k] = f[k];
+  __syncwarp();
+  mlp_forward_warp(m, xs[warp], ys[warp]);
+  if (!valid) return;
+  float y[MLP_OUT];
+  for (int o = 0; o < MLP_OUT; ++o)
+    y[o] = mlp_clip(ys[warp][lane * MLP_OUT + o]) * m.blob[MLP_OFF_OSTD + o] + m.blob[MLP_OFF_OMEAN + o];
+  double g0[NV];
+  mlp_apply(pp, y, sw, g0);
+  for (int i = 0; i < NV; ++i) guess[i * nd + t] = g0[i];
+}
+// standardised features through the tensor-core network, for kc_mlp_forward
+__global__ void __launch_bounds__(128) k_mlp_forward(MlpDev m, long n, const float* X, float* Y) {
+  __shared__ float xs[4][32 * MLP_IN];
+  __shared__ float ys[4][32 * MLP_OUT];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int k = 0; k < MLP_IN; ++k) xs[warp][lane * MLP_IN + k] = t < n ? X[t * MLP_IN + k] : 0.0f;
+  __syncwarp();
+  mlp_forward_warp(m, xs[warp], ys[warp]);
+  if (t < n)
+    for (int o = 0; o < MLP_OUT; ++o) Y[t * MLP_OUT + o] = ys[warp][lane * MLP_OUT + o];
 }
 
 // the same operator as a persistent, lane-refilling state machine (bit-identical)

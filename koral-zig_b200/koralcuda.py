@@ -26,6 +26,8 @@ KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING = 0, 1
 KC_NPASS = 14
 KC_ERR_TOO_MANY_CELLS = 9
 KC_NOALLOC_MAX_CELLS = 16384
+KC_GUESS_PLAIN, KC_GUESS_MLP = 0, 1
+KC_MLP_IN, KC_MLP_HIDDEN, KC_MLP_OUT, KC_MLP_NWEIGHTS = 16, 64, 4, 5548
 
 
 class KcScalarRow(ctypes.Structure):
@@ -129,6 +131,13 @@ def lib():
     L.kc_pass_name.restype = ctypes.c_char_p
     L.kc_get_stream.argtypes = [vp, P(vp)]
     L.kc_get_launch_count.argtypes = [vp, P(i64)]
+    L.kc_harvest_implicit.argtypes = [vp, i64]
+    L.kc_get_harvest.argtypes = [vp, vp, vp, i64, P(i64)]
+    L.kc_guess_fallbacks.argtypes = [vp]
+    L.kc_guess_fallbacks.restype = i64
+    L.kc_mlp_train.argtypes = [vp, vp, i64, i32, i32, ctypes.c_float, ctypes.c_uint64, vp, vp]
+    L.kc_mlp_forward.argtypes = [vp, i64, vp, vp]
+    L.kc_mlp_grad.argtypes = [vp, i64, vp, vp, vp, vp]
     L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
     L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
     for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
@@ -137,7 +146,8 @@ def lib():
               "kc_set_precision", "kc_set_implicit_mode", "kc_set_guess", "kc_init_puffy", "kc_implicit_batch",
               "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
               "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc", "kc_implicit_batch_device",
-              "kc_synth_implicit_cells", "kc_scalars"]:
+              "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
+              "kc_mlp_forward", "kc_mlp_grad"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -305,6 +315,31 @@ class Sim:
         self._check(self._lib.kc_init_puffy(self._h, perturb, perturb_rho, seed, ctypes.byref(fac)))
         return fac.value
 
+    # ---- the learned initial guess of the implicit solve -------------------------
+    def set_guess(self, weights=None):
+        """Install a KC_MLP_NWEIGHTS-float network (KC_GUESS_MLP), or return to
+        the reference's bisection warm start (weights None)."""
+        if weights is None:
+            self._check(self._lib.kc_set_guess(self._h, KC_GUESS_PLAIN, None, 0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(self._lib.kc_set_guess(self._h, KC_GUESS_MLP, w.ctypes.data, w.size))
+
+    def harvest_implicit(self, capacity):
+        """Collect (features, targets) of first-rung converged solves from the
+        next implicit pass on, up to `capacity` pairs (0 stops)."""
+        self._check(self._lib.kc_harvest_implicit(self._h, int(capacity)))
+
+    def get_harvest(self, capacity):
+        x = np.empty((capacity, KC_MLP_IN), dtype=np.float32)
+        t = np.empty((capacity, KC_MLP_OUT), dtype=np.float32)
+        n = ctypes.c_int64(0)
+        self._check(self._lib.kc_get_harvest(self._h, x.ctypes.data, t.ctypes.data, capacity, ctypes.byref(n)))
+        return x[:n.value].copy(), t[:n.value].copy()
+
+    def guess_fallbacks(self):
+        return int(self._lib.kc_guess_fallbacks(self._h))
+
     def debug_phase(self, phase, dt=0.0):
         self._check(self._lib.kc_debug_phase(self._h, phase, dt))
 
@@ -367,3 +402,40 @@ def u2p_batch(opt, geom23, uu, pp):
     if st != KC_OK:
         raise KoralError(st, "kc_u2p_batch")
     return pp, fl
+
+
+def _status(st, what):
+    if st != KC_OK:
+        raise KoralError(st, what)
+
+
+def mlp_train(features, targets, steps=2000, batch=1024, lr=1e-3, seed=1):
+    """Train the guess network on the GPU; returns (weights blob, loss per step)."""
+    x = np.ascontiguousarray(features, dtype=np.float32)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    w = np.empty(KC_MLP_NWEIGHTS, dtype=np.float32)
+    loss = np.empty(max(steps, 1), dtype=np.float32)
+    _status(lib().kc_mlp_train(x.ctypes.data, t.ctypes.data, x.shape[0], steps, batch, lr, seed, w.ctypes.data,
+                               loss.ctypes.data), "kc_mlp_train")
+    return w, loss[:steps]
+
+
+def mlp_forward(weights, features_std):
+    """The tensor-core forward pass on standardised features (n x 16)."""
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    x = np.ascontiguousarray(features_std, dtype=np.float32)
+    y = np.empty((x.shape[0], KC_MLP_OUT), dtype=np.float32)
+    _status(lib().kc_mlp_forward(w.ctypes.data, x.shape[0], x.ctypes.data, y.ctypes.data), "kc_mlp_forward")
+    return y
+
+
+def mlp_grad(weights, features_std, targets_std):
+    """(loss, gradient blob) of the training kernels over all pairs."""
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    x = np.ascontiguousarray(features_std, dtype=np.float32)
+    t = np.ascontiguousarray(targets_std, dtype=np.float32)
+    g = np.empty(KC_MLP_NWEIGHTS, dtype=np.float32)
+    loss = ctypes.c_float(0.0)
+    _status(lib().kc_mlp_grad(w.ctypes.data, x.shape[0], x.ctypes.data, t.ctypes.data, g.ctypes.data,
+                              ctypes.byref(loss)), "kc_mlp_grad")
+    return float(loss.value), g

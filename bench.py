@@ -369,6 +369,93 @@ def run_precision(args, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_guess(args, rank, local):
+    """The learned initial guess: (pre-solve, converged) pairs harvested from the
+    implicit passes of the 192x180x64 wedge, the network trained on the GPU,
+    then the 256x256x128 wedge stepped with the reference's bisection warm
+    start (plain), with the learned guess, and with the reference's own
+    no-bisection start, on one dt sequence: zone-cycles/s, implicit-pass time,
+    Newton iterations per solve, and the field-scale deviation of the final
+    state from the plain run's."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    kc = load_engine()
+    src = kc.Sim(kc.puffy_grid(192, 180, 64), kc.puffy_options(device=local))
+    src.initPuffy(1e-3, 1e-3, args.seed)
+    src.harvest_implicit(args.pairs)
+    hsteps = 0
+    while True:
+        src.step()
+        hsteps += 1
+        x, t = src.get_harvest(args.pairs)
+        if x.shape[0] >= args.pairs or hsteps >= 20:
+            break
+    src.close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    w, loss = kc.mlp_train(x, t, steps=args.train_steps, batch=1024, lr=2e-3, seed=3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+
+    grid = kc.puffy_grid(args.nx, args.ny, args.nz)
+    ncell = args.nx * args.ny * args.nz
+    forms = (("plain", {}, False), ("learned", {}, True), ("no_bisect", {"radimp_start_with_bisect": 0}, False))
+    out, dts, finals = {}, [], {}
+    for name, o, learned in forms:
+        sim = kc.Sim(grid, kc.puffy_options(device=local, **o))
+        sim.initPuffy(1e-3, 1e-3, args.seed)
+        if learned:
+            sim.set_guess(w)
+        k = 0
+        for _ in range(args.warmup):
+            if name == "plain":
+                dts.append(sim.step())
+            else:
+                sim.step(dts[k])
+            k += 1
+        stream = torch.cuda.ExternalStream(sim.stream())
+        c0 = sim.counters()
+        sim.set_pass_timing(True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            if name == "plain":
+                dts.append(sim.step())
+            else:
+                sim.step(dts[k])
+            k += 1
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        c1 = sim.counters()
+        solves = c1["n_radimp_solves"] - c0["n_radimp_solves"]
+        out[name] = {"value": ncell * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "implicit_ms_per_step": sim.pass_times()["implicit"][0] / args.steps,
+                     "newton_iters_per_solve": (c1["n_radimp_iters"] - c0["n_radimp_iters"]) / max(solves, 1),
+                     "solve_failures": c1["n_radimp_failures"] - c0["n_radimp_failures"]}
+        if learned:
+            out[name]["fallbacks_to_plain"] = sim.guess_fallbacks()
+        finals[name] = sim.p
+        sim.close()
+    b = finals["plain"]
+    ok = np.all(np.isfinite(b), axis=1)
+    names = ["rho", "uu", "vx", "vy", "vz", "entr", "b1", "b2", "b3", "ee", "fx", "fy", "fz"]
+    for name in ("learned", "no_bisect"):
+        d = np.abs(finals[name][ok] - b[ok]).max(axis=0) / np.maximum(np.abs(b[ok]).max(axis=0), 1e-300)
+        out[name]["field_scale_dev_vs_plain"] = dict(zip(names, d.tolist()))
+    line = {"metric": METRIC, "unit": UNIT, "workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz}, learned guess",
+            "steps": args.steps, "warmup": args.warmup, "dtype": "f64 solve, bf16 network",
+            "training": {"pairs": int(x.shape[0]), "harvest_steps": hsteps, "source": "PUFFY 3D wedge 192x180x64",
+                         "train_steps": args.train_steps, "batch": 1024, "seconds": train_s,
+                         "loss_first10": float(loss[:10].mean()), "loss_last100": float(loss[-100:].mean())},
+            **out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -381,9 +468,12 @@ def main():
     ap.add_argument("--seed", type=int, default=20250)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="step", choices=["step", "implicit", "precision"],
+    ap.add_argument("--workload", default="step", choices=["step", "implicit", "precision", "guess"],
                     help="step: the RK2IMEX step on the wedge; implicit: the batched implicit-solve microbenchmark; "
-                         "precision: mixed vs plain FP64 error study on the wedge")
+                         "precision: mixed vs plain FP64 error study on the wedge; guess: the learned initial "
+                         "guess against the plain one (use --nx 256 --ny 256 --nz 128)")
+    ap.add_argument("--pairs", type=int, default=1000000, help="training pairs of the guess workload")
+    ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
     ap.add_argument("--implicit-mode", default="per-cell", choices=["per-cell", "compacting"],
                     help="implicit solve form: one thread per cell, or the persistent lane-refilling state machine")
@@ -397,6 +487,8 @@ def main():
         return run_implicit(args, rank, world, local)
     if args.workload == "precision":
         return run_precision(args, rank, local)
+    if args.workload == "guess":
+        return run_guess(args, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

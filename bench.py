@@ -196,7 +196,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-IMPLICIT_MODES = {"per-cell": 0, "compacting": 1}
+IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2}
 IMPL_METRIC = "implicit M1 solves/s (batched, independent cells)"
 IMPL_UNIT = "solves/s"
 
@@ -475,8 +475,9 @@ def main():
     ap.add_argument("--pairs", type=int, default=1000000, help="training pairs of the guess workload")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
-    ap.add_argument("--implicit-mode", default="per-cell", choices=["per-cell", "compacting"],
-                    help="implicit solve form: one thread per cell, or the persistent lane-refilling state machine")
+    ap.add_argument("--implicit-mode", default="per-cell", choices=["per-cell", "compacting", "split"],
+                    help="implicit solve form: one thread per cell, the persistent lane-refilling state machine, or the "
+                         "split opening + compacted-ladder pair")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 3 if args.workload == "implicit" else 20

@@ -533,6 +533,27 @@ KC_HD double implicit_start_residual(const double uu00[NV], const RadState& stat
   return implicit_residual(uu, pp, st, uu00, state00, dt, g, op, whichprim, EQ_ENERGY, FRAME_LAB, f);
 }
 
+// The opening of rung 0 of the ladder (level 0, start fluid, energy equation,
+// lab frame) from a prepared state: returns 1 when the core's first exit is
+// taken there (first residual below conv), with pp and uu finished exactly as
+// implicit_ladder finishes them (the core's iteration count is then 1), else 0
+// with pp and uu untouched. The split form of the implicit pass runs this for
+// every cell and the full ladder only for the cells it leaves.
+KC_HDN int implicit_first_exit(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
+                               const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
+                               const ImplicitPre& pre) {
+  OpacParams opl = op;
+  opl.opdamp = 1.0;
+  int p, e, fr;
+  implicit_rung(0, pre.startwith, p, e, fr);
+  double pc[NV];
+  double e0 = implicit_start_residual(pre.uu00, pre.state00, pre.pp0, g, dt, gam, rad, opl, ip, p, pc);
+  if (!(e0 < ip.conv)) return 0;
+  for (int i = 0; i < NV; ++i) pp[i] = pc[i];
+  p2u(pc, uu, g, gam);
+  return 1;
+}
+
 // The same ladder started from a learned state in place of the bisection warm
 // start (the learned-guess form; it has no counterpart in the reference).
 // The start fluid is decided as solve_implicit_lab decides it. A cell the
@@ -551,8 +572,10 @@ KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], cons
   double ehat = -calc_ff_rtt(pp, g, nullptr);
   fill_rad_state(pp, g, gam, op, true, pre.state00);
   pre.startwith = (ehat < ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
+  OpacParams opl = op;
+  opl.opdamp = 1.0;
   double pc[NV];
-  double e0 = implicit_start_residual(pre.uu00, pre.state00, pp, g, dt, gam, rad, op, ip, pre.startwith, pc);
+  double e0 = implicit_start_residual(pre.uu00, pre.state00, pp, g, dt, gam, rad, opl, ip, pre.startwith, pc);
   if (e0 < ip.conv) {
     // the core's first exit on rung 0 (lab frame, energy equation)
     ImplicitResult res;
@@ -566,7 +589,7 @@ KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], cons
     res.whichframe = FRAME_LAB;
     return res;
   }
-  double e1 = implicit_start_residual(pre.uu00, pre.state00, guess, g, dt, gam, rad, op, ip, pre.startwith, pc);
+  double e1 = implicit_start_residual(pre.uu00, pre.state00, guess, g, dt, gam, rad, opl, ip, pre.startwith, pc);
   bool learned = e1 < e0;
   for (int i = 0; i < NV; ++i) pre.pp0[i] = learned ? guess[i] : pp[i];
   return implicit_ladder(uu, pp, g, dt, gam, rad, op, ip, pre);

@@ -45,7 +45,13 @@ enum {
 enum { KC_BC_PERIODIC = 0, KC_BC_COPY = 1, KC_BC_PUFFY = 2 };
 enum { KC_PLAIN_FP64 = 0, KC_MIXED = 1 };
 enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
-enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1 };
+/* implicit pass forms (no reference counterpart; all bit-identical to the
+ * reference's per-cell solveImplicitLab loop, koral/sim.zig:1715):
+ * PER_CELL one thread per cell; COMPACTING a persistent lane-refilling state
+ * machine; SPLIT an opening kernel that finishes every cell passing the Newton
+ * core's first residual test at its warm start and a ladder kernel over the
+ * compacted rest */
+enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1, KC_IMPLICIT_SPLIT = 2 };
 
 /* Pass ids of the per-pass timers, the members of koral/sim/timers.zig:4
  * Pass that the device step has. KC_PASS_FLUXES covers the reference's
@@ -114,7 +120,7 @@ typedef struct kc_options {
   int32_t bc_x, bc_y, bc_z;
   /* engine forms (no reference counterpart) */
   int32_t precision;     /* KC_PLAIN_FP64 | KC_MIXED */
-  int32_t implicit_mode; /* KC_IMPLICIT_PER_CELL | KC_IMPLICIT_COMPACTING */
+  int32_t implicit_mode; /* KC_IMPLICIT_PER_CELL | KC_IMPLICIT_COMPACTING | KC_IMPLICIT_SPLIT */
   int32_t device;        /* CUDA device ordinal */
 } kc_options;
 

@@ -60,6 +60,11 @@ struct kc_handle {
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
   int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
+  // the split form's list of cells left by the opening kernel
+  unsigned long long* split_count = nullptr;
+  int* split_cell = nullptr;
+  double* split_pp0 = nullptr;
+  int split_blocks = 0;  // resident blocks of the ladder kernel
   // the learned initial guess (KC_GUESS_MLP): FP32 blob, BF16 weight copies,
   // the per-cell seeded starts, and the training-pair harvest buffers
   int guess_mode = KC_GUESS_PLAIN;
@@ -363,6 +368,28 @@ void launch_implicit(kc_handle* h, double dtin) {
   PassScope ps(h, KC_PASS_IMPLICIT);
   // the learned guess and the harvest run in the per-cell form
   bool extra = h->guess_mode == KC_GUESS_MLP || h->hcap > 0;
+  if (h->opt.implicit_mode == KC_IMPLICIT_SPLIT && !extra) {
+    long ndom = (long)gr.nx * gr.ny * gr.nz;
+    if (!h->split_count) {
+      int st = 0;
+      h->split_count = dalloc<unsigned long long>(h, 1, st);
+      h->split_cell = dalloc<int>(h, ndom, st);
+      h->split_pp0 = dalloc<double>(h, (size_t)NV * ndom, st);
+      if (st) return;
+      int dev = 0, nsm = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_implicit_ladder, TPB, 0);
+      h->split_blocks = (per_sm > 0 ? per_sm : 1) * (nsm > 0 ? nsm : 1);
+    }
+    SplitList L = {h->split_count, h->split_cell, h->split_pp0, ndom};
+    cudaMemsetAsync(h->split_count, 0, sizeof(unsigned long long), h->stream);
+    ++h->n_launch;
+    k_implicit_open<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, L);
+    ++h->n_launch;
+    k_implicit_ladder<<<h->split_blocks, TPB, 0, h->stream>>>(h->ds, h->dsc, a, L);
+    return;
+  }
   if (h->opt.implicit_mode == KC_IMPLICIT_COMPACTING && !extra) {
     long nwork = (long)gr.nx * (gr.ny - 2L * a.polar_nc) * gr.nz;
     if (h->impl_blocks == 0) {
@@ -1040,7 +1067,7 @@ int kc_set_precision(kc_handle* h, int32_t mode) {
 }
 int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING)
+  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING && mode != KC_IMPLICIT_SPLIT)
     return fail(h, KC_ERR_INVALID_CONFIG, "unknown implicit mode");
   h->opt.implicit_mode = mode;
   return KC_OK;

@@ -904,6 +904,82 @@ __global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, Im
   }
 }
 
+// The split form of the implicit pass, bit-identical to k_implicit. Most cells
+// of a torus step pass the Newton core's first residual test at their warm
+// start, while the rest need one or more Newton iterations; in one kernel every
+// warp holding a cell of the second kind runs at that cell's pace. The opening
+// kernel runs the warm start and the rung-0 first residual for every cell,
+// finishes the cells that pass, and appends the others (domain index and warm
+// start) to a compact list; the ladder kernel runs the full ladder over the
+// list only, so its warps hold only cells that iterate.
+struct SplitList {
+  unsigned long long* count;  // cells appended by the opening kernel
+  int* cell;                  // domain index ix + nx (iy + ny iz)
+  double* pp0;                // [NV][capacity] warm starts
+  long cap;
+};
+__global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* sc, ImplArgs a, SplitList L) {
+  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+  long ix, iy, iz;
+  if (!range_cell(r, ix, iy, iz)) return;
+  if (a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) return;
+  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  double uu[NV], pp[NV];
+  load_cell(s.u, nc, c, uu);
+  load_cell(s.p, nc, c, pp);
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  ImplicitPre pre;
+  implicit_prepare(pp, g, a.dt, a.gam, a.op, a.ip, pre);
+  if (implicit_first_exit(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip, pre)) {
+    store_cell(s.u, nc, c, uu);
+    store_cell(s.p, nc, c, pp);
+    s.flags[5 * nc + c] = 0;
+    atomicAdd(&sc->n_iters, 1ULL);
+    atomicAdd(&sc->n_solves, 1ULL);
+    return;
+  }
+  unsigned long long k = atomicAdd(L.count, 1ULL);
+  if ((long)k >= L.cap) {  // cannot happen: the list holds every domain cell
+    set_err(sc, KC_ERR_CUDA, c);
+    return;
+  }
+  L.cell[k] = (int)(ix + s.gr.nx * (iy + s.gr.ny * iz));
+  for (int i = 0; i < NV; ++i) L.pp0[(long)i * L.cap + (long)k] = pre.pp0[i];
+}
+__global__ void __launch_bounds__(128) k_implicit_ladder(DevState s, DevScalars* sc, ImplArgs a, SplitList L) {
+  long n = (long)*L.count;
+  if (n > L.cap) n = L.cap;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+    long td = L.cell[k];
+    long ix = td % s.gr.nx, iy = (td / s.gr.nx) % s.gr.ny, iz = td / ((long)s.gr.nx * s.gr.ny);
+    long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+    double uu[NV], pp[NV];
+    load_cell(s.u, nc, c, uu);
+    load_cell(s.p, nc, c, pp);
+    Geom g;
+    geom_cell(s, ix, iy, iz, g);
+    // implicit_prepare's state for this cell, with the warm start it computed
+    ImplicitPre pre;
+    p2u(pp, pre.uu00, g, a.gam);
+    double ehat = -calc_ff_rtt(pp, g, nullptr);
+    fill_rad_state(pp, g, a.gam, a.op, true, pre.state00);
+    for (int i = 0; i < NV; ++i) pre.pp0[i] = L.pp0[(long)i * L.cap + k];
+    pre.startwith = (ehat < a.ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
+    ImplicitResult res = implicit_ladder(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip, pre);
+    if (res.ok) {
+      store_cell(s.u, nc, c, uu);
+      store_cell(s.p, nc, c, pp);
+      s.flags[5 * nc + c] = 0;
+      atomicAdd(&sc->n_iters, (unsigned long long)res.iters);
+      atomicAdd(&sc->n_solves, 1ULL);
+    } else {
+      s.flags[5 * nc + c] = -1;
+      atomicAdd(&sc->n_fail, 1ULL);
+    }
+  }
+}
+
 // The learned guess per domain cell: features of the pre-solve state,
 // standardised, through the tensor-core network (one warp per 32 cells), and
 // the seeded starting state written to guess [NV][nx ny nz].

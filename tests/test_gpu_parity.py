@@ -19,10 +19,11 @@ def _kc():
     return kc
 
 
-MODES = [0, 1]  # KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING (persistent state machine)
+MODES = [0, 1, 2]  # KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING (persistent state machine), KC_IMPLICIT_SPLIT
+BATCH_MODES = [0, 1]  # the batch entry points have the per-cell and persistent forms
 
 
-@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("mode", BATCH_MODES)
 def test_implicit_batch_bitwise_on_golden_records(mode):
     kc = _kc()
     i, _ = load_kgld("rad/rad_implicit")

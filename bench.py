@@ -94,16 +94,22 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
-def profiled_traffic(kernel):
-    """dram bytes per cell of `kernel` from the committed ncu summary, or None."""
+def profiled_figure(kernel, key):
+    """A per-cell figure (`key`: dram_bytes_per_cell, fp64_flop_per_solve) of
+    `kernel` from the committed ncu summary, or None."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_traffic.txt")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_cell:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1])
     except OSError:
         pass
     return None
+
+
+def profiled_traffic(kernel):
+    """dram bytes per cell of `kernel` from the committed ncu summary, or None."""
+    return profiled_figure(kernel, "dram_bytes_per_cell")
 
 
 class ClockSampler:
@@ -472,6 +478,10 @@ def main():
                     help="step: the RK2IMEX step on the wedge; implicit: the batched implicit-solve microbenchmark; "
                          "precision: mixed vs plain FP64 error study on the wedge; guess: the learned initial "
                          "guess against the plain one (use --nx 256 --ny 256 --nz 128)")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="launch the step's kernels eagerly instead of replaying a captured CUDA graph")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip the autotuner (implicit form and block sizes) before the timed steps")
     ap.add_argument("--pairs", type=int, default=1000000, help="training pairs of the guess workload")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
@@ -519,16 +529,28 @@ def main():
     t0 = time.perf_counter()
     fac = sim.initPuffy(1e-3, 1e-3, args.seed)
     init_s = time.perf_counter() - t0
+    if args.graph:
+        sim.set_graph(True)
     for _ in range(args.warmup):
         sim.step()
+    tune = None
+    if args.tune:
+        # the autotuner times candidates from this state and restores it
+        tune = sim.autotune(2)
+        for _ in range(2):  # the chosen form's eager step and graph capture
+            sim.step()
     stream = torch.cuda.ExternalStream(sim.stream())
 
     # ---- device-resident timing (value) ------------------------------------------
     clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
-    sim.set_pass_timing(True)
+    # pass timers record events on the stream; with the graph form they would run
+    # the steps eagerly, so the graph run takes its pass table from a separate
+    # eager window after the timed one
+    sim.set_pass_timing(not args.graph)
     n0 = sim.launch_count()
+    s0 = sim.counters()["n_radimp_solves"]
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
@@ -539,6 +561,16 @@ def main():
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     launches = sim.launch_count() - n0
+    solves = sim.counters()["n_radimp_solves"] - s0
+    pass_steps = args.steps
+    if args.graph:
+        pass_steps = min(args.steps, 5)
+        sim.set_pass_timing(True)
+        s0 = sim.counters()["n_radimp_solves"]
+        for _ in range(pass_steps):
+            sim.step()
+        torch.cuda.synchronize()
+        solves = sim.counters()["n_radimp_solves"] - s0
     passes = sim.pass_times()
     sim.set_pass_timing(False)
     ms_max = max_over_ranks(ms, dist, "cuda")
@@ -582,7 +614,8 @@ def main():
     for name, (pms, calls) in passes.items():
         if calls == 0:
             continue
-        entry = {"ms_per_step": pms / args.steps, "share": pms / total if total else 0.0, "calls_per_step": calls / args.steps}
+        entry = {"ms_per_step": pms / pass_steps, "share": pms / total if total else 0.0,
+                 "calls_per_step": calls / pass_steps}
         bpc = pass_bytes(name, ndim)
         if bpc is not None:
             entry["gbs"] = bpc * ncell / (pms / calls / 1e3) / 1e9
@@ -601,6 +634,17 @@ def main():
         "avg_launch_ms": dom_ms / dom_calls,
         "passes": table,
     }
+    # the FP64 side of the implicit solve: ncu-counted FLOP per cell-solve (dadd +
+    # dmul + 2 dfma) x this run's solves per launch over the live launch time,
+    # against the DFMA peak measured now on this device
+    fps = profiled_figure("k_implicit", "fp64_flop_per_solve")
+    if dom == "implicit" and fps:
+        solves_per_launch = solves / max(dom_calls, 1)
+        peak64 = kc.fp64_peak()
+        got = fps * solves_per_launch / (dom_ms / dom_calls / 1e3) / 1e12
+        roofline["fp64"] = {"achieved": got, "peak": peak64, "unit": "TFLOP/s", "frac": got / peak64,
+                            "flop_per_solve": fps, "solves_per_launch": solves_per_launch,
+                            "peak_kind": "measured (kc_fp64_peak, DFMA chains)"}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -609,7 +653,10 @@ def main():
         "config": {"workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz} MKS2 (periodic phi), plain FP64",
                    "cells": ncell, "ghosts": 3, "precision": "plain FP64", "l2": "inputs larger than L2 (no flush)",
                    "init_seconds": init_s, "beta_norm_factor": fac, "parallelism": f"replicas x{world}",
-                   "implicit_mode": args.implicit_mode},
+                   "implicit_mode": args.implicit_mode if tune is None else
+                   {0: "per-cell", 1: "compacting", 2: "split"}[tune["implicit_mode"]],
+                   "cuda_graph": bool(args.graph), "autotune": tune,
+                   "pass_table": "timed region" if not args.graph else f"{pass_steps} eager steps after it"},
         "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": launches,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

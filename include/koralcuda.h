@@ -224,6 +224,29 @@ int kc_get_launch_count(kc_handle* h, int64_t* n);
 /* Engine forms (no reference counterpart) */
 int kc_set_precision(kc_handle* h, int32_t mode);
 int kc_set_implicit_mode(kc_handle* h, int32_t mode);
+/* The step as a CUDA graph: with on != 0 the whole step's launch sequence
+ * (every pass of koral/sim.zig:1792 step, and the copy of its dt-derived
+ * coefficients from a pinned table) is captured once and replayed each step;
+ * results are bit-identical to the eager launches. The step after a change of
+ * form (precision, implicit form, guess, harvest) runs eagerly, the next one is
+ * captured. Pass timing (kc_set_pass_timing) runs the steps eagerly. */
+int kc_set_graph(kc_handle* h, int32_t on);
+
+/* The autotuner's choice (no reference counterpart): implicit form
+ * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT) and threads per block of the
+ * per-cell implicit, face-flux and u2p kernels, with the measured step time of
+ * the choice and of the configuration on entry. */
+typedef struct kc_tune_result {
+  int32_t implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
+  double ms_per_step, ms_per_step_entry;
+  int32_t trials;
+} kc_tune_result;
+/* Times whole steps on the handle's current state for each candidate, one
+ * knob at a time, and keeps the fastest configuration set; the state and the
+ * counters are restored afterwards, and all candidates are bit-identical.
+ * `steps` timed steps per trial (after one untimed step, two with the graph
+ * form). Not with the learned guess, the harvest or pass timing on. */
+int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out);
 
 /* The learned initial guess of the implicit solve (no reference counterpart).
  * A 16 -> 64 -> 64 -> 4 ReLU network predicts, from a cell's pre-solve
@@ -270,6 +293,11 @@ int kc_mlp_train(const float* features, const float* targets, int64_t n, int32_t
 int kc_mlp_forward(const float* weights, int64_t n, const float* features_std, float* out_std);
 int kc_mlp_grad(const float* weights, int64_t n, const float* features_std, const float* targets_std, float* grad,
                 float* loss);
+
+/* The FP64 pipe's peak on the current device, measured: independent DFMA
+ * chains over every SM, best of five launches, in TFLOP/s (the denominator of
+ * the FP64 roofline of the implicit solve and u2p; no reference counterpart). */
+int kc_fp64_peak(double* tflops);
 
 /* Batched per-cell entry points over n independent cells (the C4 implicit
  * microbench and the parity harnesses). geom23 is the reference's golden

@@ -53,6 +53,9 @@ struct DevState {
   double* scaleth; // [nx]
   double* fix_p;   // [NV][nc] fixup staging
   double* fix_u;   // [NV][nc]
+  // the step's dt-derived coefficients (dt, dt gamma_imex, ...), written once a
+  // step from the host, so that a captured step graph reads each step's values
+  const double* coef;
 };
 
 // Device-side scalars written by kernels (one block, read back once a step).

@@ -60,6 +60,19 @@ struct kc_handle {
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
   int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
+  // block sizes of the per-cell implicit, face-flux and u2p kernels (kc_autotune)
+  int tpb_implicit = TPB, tpb_flux = TPB, tpb_u2p = TPB;
+  // the step's dt-derived coefficients: pinned host table and its device copy
+  // (DevState::coef); slots 0-3 are fixed by run_step, later ones appended
+  double* coef_host = nullptr;
+  double* coef_dev = nullptr;
+  int ncoef = 0;
+  DevScalars* dsc_init = nullptr;  // the step-start value of the device scalars
+  // CUDA graph of the whole step (kc_set_graph): captured once per launch
+  // sequence and replayed; any setter that changes the sequence drops it
+  bool use_graph = false, graph_warm = false;
+  cudaGraphExec_t gexec = nullptr;
+  long long graph_launches = 0;
   // the split form's list of cells left by the opening kernel
   unsigned long long* split_count = nullptr;
   int* split_cell = nullptr;
@@ -336,7 +349,7 @@ void launch_calc_u2p(kc_handle* h) {
   PassScope ps(h, KC_PASS_U2P);
   cudaMemsetAsync(&h->dsc->any_hd, 0, sizeof(int), h->stream);
   ++h->n_launch;
-  k_u2p<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, h->sp.fl, h->sp.rp, pnc);
+  k_u2p<<<nblk(ndom, h->tpb_u2p), h->tpb_u2p, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, h->sp.fl, h->sp.rp, pnc);
   if (h->sp.do_fixups) {
     PassScope pf(h, KC_PASS_FIXUP);
     ++h->n_launch;
@@ -356,11 +369,11 @@ void launch_do_correct(kc_handle* h) {
   k_polar_correct<<<nblk((long)gr.nx * gr.nz * 2 * ncp), TPB, 0, h->stream>>>(h->ds, h->sp.gam, ncp);
 }
 
-void launch_implicit(kc_handle* h, double dtin) {
+void launch_implicit(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   ImplArgs a;
   a.gam = h->sp.gam;
-  a.dt = dtin;
+  a.dt_slot = dt_slot;
   a.rp = h->sp.rp;
   a.op = h->sp.op;
   a.ip = h->sp.ip;
@@ -425,7 +438,7 @@ void launch_implicit(kc_handle* h, double dtin) {
   }
   ++h->n_launch;
   if (extra) k_implicit<true><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
-  else k_implicit<false><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  else k_implicit<false><<<nblk(ndom, h->tpb_implicit), h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
 }
 
 void launch_wavespeeds(kc_handle* h) {
@@ -459,8 +472,9 @@ void launch_face_fluxes(kc_handle* h) {
     long n1 = dims[c1] > 1 ? dims[c1] + 2 : dims[c1];
     long n = (dims[dim] + 1) * n0 * n1;
     ++h->n_launch;
-    if (h->opt.precision == KC_MIXED) k_face_flux<true><<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
-    else k_face_flux<false><<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a, dim);
+    int tb = h->tpb_flux;
+    if (h->opt.precision == KC_MIXED) k_face_flux<true><<<nblk(n, tb), tb, 0, h->stream>>>(h->ds, h->dsc, a, dim);
+    else k_face_flux<false><<<nblk(n, tb), tb, 0, h->stream>>>(h->ds, h->dsc, a, dim);
   }
 }
 
@@ -476,7 +490,7 @@ void launch_flux_ct(kc_handle* h) {
   else k_ct_rebuild<double><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
 }
 
-void launch_op_explicit(kc_handle* h, double dtin) {
+void launch_op_explicit(kc_handle* h, int dt_slot) {
   launch_wavespeeds(h);
   launch_face_fluxes(h);
   launch_flux_ct(h);
@@ -484,18 +498,18 @@ void launch_op_explicit(kc_handle* h, double dtin) {
   {
     PassScope ps(h, KC_PASS_UPDATE);
     ++h->n_launch;
-    k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dtin);
+    k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dt_slot);
   }
   launch_calc_u2p(h);
 }
 
-void launch_rijvisc(kc_handle* h, double global_dt) {
+void launch_rijvisc(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   PassScope ps(h, KC_PASS_RADVISC);
   cudaMemsetAsync(h->ds.rijvisc, 0, (size_t)16 * gr.nc * 8, h->stream);
   ViscArgs a;
   a.gam = h->sp.gam;
-  a.dt = global_dt;
+  a.dt_slot = dt_slot;
   a.rhor = r_horizon_bl(h->sp.mp.a);
   a.alpha = h->sp.alpharadvisc;
   a.op = h->sp.op;
@@ -504,7 +518,7 @@ void launch_rijvisc(kc_handle* h, double global_dt) {
   k_rijvisc<<<nblk(n), TPB, 0, h->stream>>>(h->ds, a);
 }
 
-void launch_dynamo(kc_handle* h, double dt) {
+void launch_dynamo(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   PassScope ps(h, KC_PASS_DYNAMO);
   ++h->n_launch;
@@ -512,7 +526,7 @@ void launch_dynamo(kc_handle* h, double dt) {
   launch_set_bc(h);
   DynArgs a;
   a.gam = h->sp.gam;
-  a.dt = dt;
+  a.dt_slot = dt_slot;
   a.a = h->sp.mp.a;
   a.rhor = r_horizon_bl(h->sp.mp.a);
   a.risco = r_isco_bl(h->sp.mp.a);
@@ -528,13 +542,13 @@ void launch_dynamo(kc_handle* h, double dt) {
   launch_calc_u2p(h);
 }
 
-void launch_stage_deriv(kc_handle* h, double* dst, const double* a, const double* b, double delta) {
+void launch_stage_deriv(kc_handle* h, double* dst, const double* a, const double* b, int delta) {
   const DGrid& gr = h->gr;
   PassScope ps(h, KC_PASS_STAGE);
   ++h->n_launch;
   k_stage_deriv<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds, dst, a, b, delta);
 }
-void launch_stage_combine(kc_handle* h, double* dst, const double* a, double f1, const double* b, double f2,
+void launch_stage_combine(kc_handle* h, double* dst, const double* a, int f1, const double* b, int f2,
                           const double* c) {
   const DGrid& gr = h->gr;
   PassScope ps(h, KC_PASS_STAGE);
@@ -546,12 +560,38 @@ void copy_field(kc_handle* h, double* dst, const double* src) {
   cudaMemcpyAsync(dst, src, (size_t)NV * h->gr.nc * 8, cudaMemcpyDeviceToDevice, h->stream);
 }
 
+// Coefficient slots of a step (run_step fills 0-3 before its first launch)
+enum { C_DT = 0, C_DT_GAM = 1, C_DT_1M2GAM = 2, C_DT_HALF = 3, NCOEF = 16 };
+// the slot holding v (bit-equal), appended and copied to the device if new;
+// a full table waits for the stream before it is reused (the host table is
+// pinned and read by copies when they run)
+int coef_slot(kc_handle* h, double v) {
+  for (int i = 0; i < h->ncoef; ++i)
+    if (memcmp(&h->coef_host[i], &v, 8) == 0) return i;
+  if (h->ncoef == NCOEF) {
+    cudaStreamSynchronize(h->stream);
+    h->ncoef = 0;
+  }
+  int i = h->ncoef++;
+  h->coef_host[i] = v;
+  cudaMemcpyAsync(h->coef_dev + i, h->coef_host + i, 8, cudaMemcpyHostToDevice, h->stream);
+  return i;
+}
+// the step's table: written on the host (no copy pending: the previous step
+// ended with a stream synchronize), copied by the step's first operation
+void coef_set_step(kc_handle* h, double dt) {
+  h->coef_host[C_DT] = dt;
+  h->coef_host[C_DT_GAM] = dt * KP_GAM_IMEX;
+  h->coef_host[C_DT_1M2GAM] = dt * KP_ONE_M2GAM;
+  h->coef_host[C_DT_HALF] = dt / 2.0;
+  h->ncoef = 4;
+}
+void coef_copy_step(kc_handle* h) {
+  cudaMemcpyAsync(h->coef_dev, h->coef_host, 4 * 8, cudaMemcpyHostToDevice, h->stream);
+}
+
 void reset_step_scalars(kc_handle* h) {
-  DevScalars z;
-  memset(&z, 0, sizeof(z));
-  double big = 1.0e50;
-  memcpy(&z.tsd_min_bits, &big, 8);
-  cudaMemcpyAsync(h->dsc, &z, sizeof(z), cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->dsc, h->dsc_init, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->stream);
 }
 
 // read the device scalars, fold them into the handle (sim.zig:634 reduceStepGlobals)
@@ -582,55 +622,48 @@ int collect_step_scalars(kc_handle* h, bool fold_cfl) {
   return KC_OK;
 }
 
-// Sim.step (koral/sim.zig:1792)
-int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
-  double t = h->t;
-  h->own_dt = 1.0 / h->tstepdenmax;
-  double dt = isnan(forced_dt) ? h->own_dt : forced_dt;
-  h->dt = dt;
-  long long fail0 = h->n_fail;
-  h->tstepdenmax = -1.0;
-  h->tstepdenmin = 1.0e50;
-  PassScope pstep(h, KC_PASS_STEP);
+// The launch sequence of Sim.step (koral/sim.zig:1792), coefficients from the
+// step table (C_* slots)
+void enqueue_step(kc_handle* h) {
+  coef_copy_step(h);
   reset_step_scalars(h);
-  const double gam_imex = KP_GAM_IMEX;
   double* u = h->ds.u;
-  if (h->sp.radviscosity) launch_rijvisc(h, dt);
+  if (h->sp.radviscosity) launch_rijvisc(h, C_DT);
   // 1st implicit
   copy_field(h, h->ut0, u);
-  launch_implicit(h, dt * gam_imex);
-  launch_stage_deriv(h, h->drt1, u, h->ut0, dt * gam_imex);
+  launch_implicit(h, C_DT_GAM);
+  launch_stage_deriv(h, h->drt1, u, h->ut0, C_DT_GAM);
   // 1st explicit
   copy_field(h, h->ut1, u);
   launch_calc_u2p(h);
   launch_do_correct(h);
   launch_set_bc(h);
-  launch_op_explicit(h, dt);
-  if (h->sp.dynamo) launch_dynamo(h, dt);
+  launch_op_explicit(h, C_DT);
+  if (h->sp.dynamo) launch_dynamo(h, C_DT);
   {
     const DGrid& gr = h->gr;
     PassScope ps(h, KC_PASS_STAGE);
     ++h->n_launch;
     k_copy_entropy_count<<<nblk((long)gr.nx * gr.ny * gr.nz, 256), 256, 0, h->stream>>>(h->ds);
   }
-  launch_stage_deriv(h, h->dut1, u, h->ut1, dt);
-  launch_stage_combine(h, u, h->ut0, dt, h->dut1, dt * KP_ONE_M2GAM, h->drt1);
+  launch_stage_deriv(h, h->dut1, u, h->ut1, C_DT);
+  launch_stage_combine(h, u, h->ut0, C_DT, h->dut1, C_DT_1M2GAM, h->drt1);
   // 2nd implicit
   copy_field(h, h->uforget, u);
   launch_calc_u2p(h);
   launch_do_correct(h);
-  launch_implicit(h, gam_imex * dt);
-  launch_stage_deriv(h, h->drt2, u, h->uforget, dt * gam_imex);
+  launch_implicit(h, C_DT_GAM);
+  launch_stage_deriv(h, h->drt2, u, h->uforget, C_DT_GAM);
   // 2nd explicit
   copy_field(h, h->ut2, u);
   launch_calc_u2p(h);
   launch_do_correct(h);
   launch_set_bc(h);
-  launch_op_explicit(h, dt);
-  if (h->sp.dynamo) launch_dynamo(h, dt);
-  launch_stage_deriv(h, h->dut2, u, h->ut2, dt);
-  launch_stage_combine(h, u, h->ut0, dt / 2.0, h->dut1, dt / 2.0, h->dut2);
-  launch_stage_combine(h, u, u, dt / 2.0, h->drt1, dt / 2.0, h->drt2);
+  launch_op_explicit(h, C_DT);
+  if (h->sp.dynamo) launch_dynamo(h, C_DT);
+  launch_stage_deriv(h, h->dut2, u, h->ut2, C_DT);
+  launch_stage_combine(h, u, h->ut0, C_DT_HALF, h->dut1, C_DT_HALF, h->dut2);
+  launch_stage_combine(h, u, u, C_DT_HALF, h->drt1, C_DT_HALF, h->drt2);
   launch_calc_u2p(h);
   launch_do_correct(h);
   launch_set_bc(h);
@@ -640,8 +673,65 @@ int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
     ++h->n_launch;
     k_update_entropy<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam);
   }
+}
+
+void drop_graph(kc_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->gexec = nullptr;
+  h->graph_warm = false;
+}
+
+// Enqueues one step: eagerly, or as a replay of the captured step graph. The
+// graph holds the coefficient copy from the pinned table, so a replay runs
+// with the values coef_set_step wrote. After any change of the launch sequence
+// one step runs eagerly (lazy allocations happen outside a capture), the next
+// one is captured, and later ones replay it.
+int launch_step(kc_handle* h) {
+  bool graph = h->use_graph && !h->timing;
+  if (!graph) {
+    enqueue_step(h);
+    return KC_OK;
+  }
+  if (h->gexec) {
+    h->n_launch += h->graph_launches;
+    return cuda_check(h, cudaGraphLaunch(h->gexec, h->stream), "graph launch");
+  }
+  if (!h->graph_warm) {
+    enqueue_step(h);
+    h->graph_warm = true;
+    return KC_OK;
+  }
+  int st = cuda_check(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+  if (st) return st;
+  long long n0 = h->n_launch;
+  enqueue_step(h);
+  cudaGraph_t g = nullptr;
+  st = cuda_check(h, cudaStreamEndCapture(h->stream, &g), "graph capture");
+  if (!st) st = cuda_check(h, cudaGraphInstantiate(&h->gexec, g, 0), "graph instantiate");
+  if (g) cudaGraphDestroy(g);
+  if (st) {
+    h->gexec = nullptr;
+    return st;
+  }
+  h->graph_launches = h->n_launch - n0;
+  return cuda_check(h, cudaGraphLaunch(h->gexec, h->stream), "graph launch");
+}
+
+// Sim.step (koral/sim.zig:1792)
+int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
+  double t = h->t;
+  h->own_dt = 1.0 / h->tstepdenmax;
+  double dt = isnan(forced_dt) ? h->own_dt : forced_dt;
+  h->dt = dt;
+  long long fail0 = h->n_fail;
+  h->tstepdenmax = -1.0;
+  h->tstepdenmin = 1.0e50;
+  coef_set_step(h, dt);
+  PassScope pstep(h, KC_PASS_STEP);
+  int st = launch_step(h);
   pstep.end();
-  int st = sync_check(h, "step launch");
+  if (st) return st;
+  st = sync_check(h, "step launch");
   if (st) return st;
   st = collect_step_scalars(h, true);
   if (h->timing) pass_collect(h);
@@ -729,8 +819,20 @@ int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
   h->staging = dalloc<double>(h, NV * nc, st);
   h->flag_staging = dalloc<int>(h, 6 * nc, st);
   h->dsc = dalloc<DevScalars>(h, 1, st);
+  h->dsc_init = dalloc<DevScalars>(h, 1, st);
   h->diag = dalloc<double>(h, 16, st);
+  h->coef_dev = dalloc<double>(h, NCOEF, st);
   if (st) return st;
+  if (cudaMallocHost(&h->coef_host, NCOEF * 8) != cudaSuccess) return fail(h, KC_ERR_OOM, "cudaMallocHost");
+  memset(h->coef_host, 0, NCOEF * 8);
+  h->ds.coef = h->coef_dev;
+  {
+    DevScalars z;
+    memset(&z, 0, sizeof(z));
+    double big = 1.0e50;
+    memcpy(&z.tsd_min_bits, &big, 8);
+    if ((st = cuda_check(h, cudaMemcpy(h->dsc_init, &z, sizeof(z), cudaMemcpyHostToDevice), "create"))) return st;
+  }
   // set_grid min-size scan with C's mdx quirk (koral/sim.zig:443)
   double mdx = -1, mdy = -1, mdz = -1;
   for (long ix = 0; ix < g.nx; ++ix)
@@ -749,6 +851,9 @@ int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
 
 void kc_destroy(kc_handle* h) {
   if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graph(h);
+  if (h->coef_host) cudaFreeHost(h->coef_host);
   for (void* p : h->allocs) cudaFree(p);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1027,15 +1132,15 @@ int kc_debug_phase(kc_handle* h, int phase, double dt) {
     case 3: {
       const DGrid& gr = h->gr;
       ++h->n_launch;
-      k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, dt);
+      k_update<<<nblk((long)gr.nx * gr.ny * gr.nz), TPB, 0, h->stream>>>(h->ds, h->sp.gam, coef_slot(h, dt));
       break;
     }
     case 4: launch_calc_u2p(h); break;
-    case 5: launch_implicit(h, dt); break;
-    case 6: launch_rijvisc(h, dt); break;
-    case 7: launch_dynamo(h, dt); break;
+    case 5: launch_implicit(h, coef_slot(h, dt)); break;
+    case 6: launch_rijvisc(h, coef_slot(h, dt)); break;
+    case 7: launch_dynamo(h, coef_slot(h, dt)); break;
     case 8: launch_do_correct(h); break;
-    case 9: launch_op_explicit(h, dt); break;
+    case 9: launch_op_explicit(h, coef_slot(h, dt)); break;
     default: return KC_ERR_INVALID_CONFIG;
   }
   int st = sync_check(h, "phase");
@@ -1063,6 +1168,7 @@ int kc_set_precision(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   if (mode != KC_PLAIN_FP64 && mode != KC_MIXED) return fail(h, KC_ERR_INVALID_CONFIG, "unknown precision mode");
   h->opt.precision = mode;
+  drop_graph(h);
   return KC_OK;
 }
 int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
@@ -1070,6 +1176,7 @@ int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
   if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING && mode != KC_IMPLICIT_SPLIT)
     return fail(h, KC_ERR_INVALID_CONFIG, "unknown implicit mode");
   h->opt.implicit_mode = mode;
+  drop_graph(h);
   return KC_OK;
 }
 static int ensure_imp_ctr(kc_handle* h) {
@@ -1077,10 +1184,20 @@ static int ensure_imp_ctr(kc_handle* h) {
   if (!h->imp_ctr) h->imp_ctr = dalloc<unsigned long long>(h, 2, st);
   return st;
 }
+// The CUDA graph form of the step (no reference counterpart): on, the whole
+// step's launch sequence is captured once and replayed (bit-identical).
+int kc_set_graph(kc_handle* h, int32_t on) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graph(h);
+  h->use_graph = on != 0;
+  return KC_OK;
+}
 int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweights) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   if (mode == KC_GUESS_PLAIN) {
     h->guess_mode = KC_GUESS_PLAIN;
+    drop_graph(h);
     return KC_OK;
   }
   if (mode != KC_GUESS_MLP) return fail(h, KC_ERR_INVALID_CONFIG, "unknown guess mode");
@@ -1108,6 +1225,7 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
   e = cuda_check(h, cudaStreamSynchronize(h->stream), "guess pack");
   if (e) return e;
   h->guess_mode = KC_GUESS_MLP;
+  drop_graph(h);
   return KC_OK;
 }
 int kc_harvest_implicit(kc_handle* h, int64_t capacity) {
@@ -1120,6 +1238,7 @@ int kc_harvest_implicit(kc_handle* h, int64_t capacity) {
     if (st) return st;
   }
   h->hcap = capacity;
+  drop_graph(h);
   return cuda_check(h, cudaMemsetAsync(h->imp_ctr + 1, 0, 8, h->stream), "harvest reset");
 }
 int kc_get_harvest(kc_handle* h, float* features, float* targets, int64_t capacity, int64_t* n_out) {
@@ -1739,6 +1858,187 @@ extern "C" int kc_mlp_train(const float* features, const float* targets, int64_t
     std::vector<float> l(steps);
     cudaMemcpy(l.data(), dl.p, steps * 4, cudaMemcpyDeviceToHost);
     for (int s = 0; s < steps; ++s) loss_curve[s] = l[s] / (float)(nb * MLP_OUT);
+  }
+  return KC_OK;
+}
+
+// ---- FP64 pipe peak: a DFMA-chain microbenchmark (the FP64 roofline) -------------
+namespace {
+const int DFMA_CHAINS = 16;
+__global__ void __launch_bounds__(256) k_dfma_chains(double* sink, int iters, double b, double c) {
+  double a[DFMA_CHAINS];
+  for (int k = 0; k < DFMA_CHAINS; ++k) a[k] = 1.0e-3 * (threadIdx.x + k);
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int k = 0; k < DFMA_CHAINS; ++k) a[k] = __fma_rn(a[k], b, c);
+  double s = 0.0;
+  for (int k = 0; k < DFMA_CHAINS; ++k) s += a[k];
+  if (s == -1.0) sink[blockIdx.x] = s;  // never true; keeps the chains live
+}
+}  // namespace
+
+// Best of five launches of independent DFMA chains over every SM, in TFLOP/s
+// (2 FLOP per DFMA). Runs on the current device.
+extern "C" int kc_fp64_peak(double* tflops) {
+  int st = mlp_device();
+  if (st) return st;
+  if (!tflops) return KC_ERR_INVALID_CONFIG;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = nsm * 8, threads = 256, iters = 1 << 14;
+  DevBuf sink;
+  if (cudaMalloc(&sink.p, (size_t)blocks * 8)) return KC_ERR_OOM;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_dfma_chains<<<blocks, threads>>>((double*)sink.p, 256, 0.999999, 1.0e-7);
+  float best = 1.0e30f;
+  for (int r = 0; r < 5; ++r) {
+    cudaEventRecord(e0);
+    k_dfma_chains<<<blocks, threads>>>((double*)sink.p, iters, 0.999999, 1.0e-7);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (cudaGetLastError() != cudaSuccess) return KC_ERR_CUDA;
+  *tflops = 2.0 * DFMA_CHAINS * (double)iters * blocks * threads / (best * 1.0e-3) / 1.0e12;
+  return KC_OK;
+}
+
+// ---- autotuner -------------------------------------------------------------------
+namespace {
+struct TuneConfig {
+  int implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
+};
+void tune_apply(kc_handle* h, const TuneConfig& c) {
+  h->opt.implicit_mode = c.implicit_mode;
+  h->tpb_implicit = c.tpb_implicit;
+  h->tpb_flux = c.tpb_flux;
+  h->tpb_u2p = c.tpb_u2p;
+  drop_graph(h);
+}
+TuneConfig tune_current(const kc_handle* h) {
+  return {h->opt.implicit_mode, h->tpb_implicit, h->tpb_flux, h->tpb_u2p};
+}
+// The state a step reads and writes across steps: p, u, flags on the device and
+// the handle's step scalars and counters.
+struct TuneSnapshot {
+  double *p = nullptr, *u = nullptr;
+  int* flags = nullptr;
+  kc_counters c;
+  long long n_launch = 0;
+};
+void tune_save(kc_handle* h, TuneSnapshot& sn) {
+  size_t nb = (size_t)NV * h->gr.nc * 8;
+  cudaMemcpyAsync(sn.p, h->ds.p, nb, cudaMemcpyDeviceToDevice, h->stream);
+  cudaMemcpyAsync(sn.u, h->ds.u, nb, cudaMemcpyDeviceToDevice, h->stream);
+  cudaMemcpyAsync(sn.flags, h->ds.flags, (size_t)6 * h->gr.nc * 4, cudaMemcpyDeviceToDevice, h->stream);
+  kc_get_counters(h, &sn.c);
+  sn.n_launch = h->n_launch;
+}
+void tune_restore(kc_handle* h, const TuneSnapshot& sn) {
+  size_t nb = (size_t)NV * h->gr.nc * 8;
+  cudaMemcpyAsync(h->ds.p, sn.p, nb, cudaMemcpyDeviceToDevice, h->stream);
+  cudaMemcpyAsync(h->ds.u, sn.u, nb, cudaMemcpyDeviceToDevice, h->stream);
+  cudaMemcpyAsync(h->ds.flags, sn.flags, (size_t)6 * h->gr.nc * 4, cudaMemcpyDeviceToDevice, h->stream);
+  kc_set_counters(h, &sn.c);
+  h->n_launch = sn.n_launch;
+}
+}  // namespace
+
+// Picks the implicit form (per-cell or split) and the block sizes of the
+// per-cell implicit, face-flux and u2p kernels by timing whole steps on the
+// handle's current state, one knob at a time (coordinate descent from the
+// configuration on entry). Each trial restores the state, runs one untimed step
+// (with the graph form on, a second one, so the timed steps replay the graph)
+// and times `steps` steps with CUDA events on the handle's stream. Every
+// candidate gives bit-identical results, so the choice changes speed only. The
+// state and counters are restored at the end, and the best configuration stays
+// set. The learned guess and the harvest keep their fixed forms (not tuned
+// while either is on).
+extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
+  if (!h || steps < 1) return KC_ERR_INVALID_CONFIG;
+  if (h->last_status) return h->last_status;
+  if (h->guess_mode != KC_GUESS_PLAIN || h->hcap > 0)
+    return fail(h, KC_ERR_INVALID_CONFIG, "autotune with the learned guess or the harvest on");
+  if (h->timing) return fail(h, KC_ERR_INVALID_CONFIG, "autotune with pass timing on");
+  int st = cuda_check(h, cudaStreamSynchronize(h->stream), "autotune");
+  if (st) return st;
+  TuneSnapshot sn;
+  size_t nb = (size_t)NV * h->gr.nc * 8;
+  if (cudaMalloc(&sn.p, nb) || cudaMalloc(&sn.u, nb) || cudaMalloc(&sn.flags, (size_t)6 * h->gr.nc * 4)) {
+    cudaFree(sn.p);
+    cudaFree(sn.u);
+    cudaFree(sn.flags);
+    return fail(h, KC_ERR_OOM, "autotune snapshot");
+  }
+  tune_save(h, sn);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int trials = 0;
+  auto measure = [&](const TuneConfig& c, double& ms) -> int {
+    tune_restore(h, sn);
+    tune_apply(h, c);
+    int warm = h->use_graph ? 2 : 1;
+    for (int k = 0; k < warm; ++k)
+      if (int r = run_step(h, NAN, nullptr)) return r;
+    cudaEventRecord(e0, h->stream);
+    for (int k = 0; k < steps; ++k)
+      if (int r = run_step(h, NAN, nullptr)) return r;
+    cudaEventRecord(e1, h->stream);
+    cudaEventSynchronize(e1);
+    float f = 0.0f;
+    cudaEventElapsedTime(&f, e0, e1);
+    ms = f / steps;
+    ++trials;
+    return KC_OK;
+  };
+  TuneConfig best = tune_current(h), entry = best;
+  double best_ms = 0.0, entry_ms = 0.0;
+  st = measure(best, best_ms);
+  entry_ms = best_ms;
+  const int forms[2] = {KC_IMPLICIT_PER_CELL, KC_IMPLICIT_SPLIT};
+  const int sizes[3] = {64, 96, 128};
+  for (int knob = 0; knob < 4 && !st; ++knob) {
+    int n = knob == 0 ? 2 : 3;
+    for (int i = 0; i < n && !st; ++i) {
+      TuneConfig c = best;
+      if (knob == 0) c.implicit_mode = forms[i];
+      if (knob == 1) c.tpb_implicit = sizes[i];
+      if (knob == 2) c.tpb_flux = sizes[i];
+      if (knob == 3) c.tpb_u2p = sizes[i];
+      if (memcmp(&c, &best, sizeof c) == 0) continue;
+      double ms = 0.0;
+      st = measure(c, ms);
+      if (!st && ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+  }
+  tune_restore(h, sn);
+  tune_apply(h, st ? entry : best);
+  cudaStreamSynchronize(h->stream);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sn.p);
+  cudaFree(sn.u);
+  cudaFree(sn.flags);
+  if (st) return st;
+  if (out) {
+    out->implicit_mode = best.implicit_mode;
+    out->tpb_implicit = best.tpb_implicit;
+    out->tpb_flux = best.tpb_flux;
+    out->tpb_u2p = best.tpb_u2p;
+    out->ms_per_step = best_ms;
+    out->ms_per_step_entry = entry_ms;
+    out->trials = trials;
   }
   return KC_OK;
 }

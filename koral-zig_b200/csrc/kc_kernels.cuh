@@ -61,7 +61,8 @@ __global__ void k_flags_to_aos(const int* __restrict__ soa, int* __restrict__ ao
 
 // ---- stage arithmetic (koral/sim.zig:1586-1709) ------------------------------
 // dst = (1/delta) a + (-1/delta) b over the domain
-__global__ void k_stage_deriv(DevState s, double* dst, const double* a, const double* b, double delta) {
+__global__ void k_stage_deriv(DevState s, double* dst, const double* a, const double* b, int delta_slot) {
+  const double delta = s.coef[delta_slot];
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
   if (!range_cell(r, ix, iy, iz)) return;
@@ -72,8 +73,9 @@ __global__ void k_stage_deriv(DevState s, double* dst, const double* a, const do
   for (int iv = 0; iv < NV; ++iv) dst[iv * nc + c] = f1 * a[iv * nc + c] + f2 * b[iv * nc + c];
 }
 // dst = a + f1 b + f2 cc over the domain
-__global__ void k_stage_combine(DevState s, double* dst, const double* a, double f1, const double* b, double f2,
+__global__ void k_stage_combine(DevState s, double* dst, const double* a, int f1_slot, const double* b, int f2_slot,
                                 const double* cc) {
+  const double f1 = s.coef[f1_slot], f2 = s.coef[f2_slot];
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
   if (!range_cell(r, ix, iy, iz)) return;
@@ -795,7 +797,7 @@ __global__ void k_ct_rebuild(DevState s) {
 }
 
 // ---- conserved update + metric source (sim.zig:1140,1542) --------------------
-__global__ void __launch_bounds__(128) k_update(DevState s, double gam, double dtin) {
+__global__ void __launch_bounds__(128) k_update(DevState s, double gam, int dt_slot) {
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
   if (!range_cell(r, ix, iy, iz)) return;
@@ -822,7 +824,7 @@ __global__ void __launch_bounds__(128) k_update(DevState s, double gam, double d
         ss[rrows[nu]] += gdetu * rl[a][l] * k;
       }
   double dx = cell_size(g, ix, 0), dy = cell_size(g, iy, 1), dz = cell_size(g, iz, 2);
-  double dt = dtin;
+  double dt = s.coef[dt_slot];
   long fx0 = face_index(s.gr, 0, ix, iy, iz), fx1 = face_index(s.gr, 0, ix + 1, iy, iz);
   long fy0 = face_index(s.gr, 1, ix, iy, iz), fy1 = face_index(s.gr, 1, ix, iy + 1, iz);
   long fz0 = face_index(s.gr, 2, ix, iy, iz), fz1 = face_index(s.gr, 2, ix, iy, iz + 1);
@@ -838,7 +840,8 @@ __global__ void __launch_bounds__(128) k_update(DevState s, double gam, double d
 
 // ---- implicit operator (sim.zig:1715) ----------------------------------------
 struct ImplArgs {
-  double gam, dt;
+  double gam;
+  int dt_slot;  // the pass's dt in DevState::coef
   RadParams rp;
   OpacParams op;
   ImplicitParams ip;
@@ -857,6 +860,7 @@ struct ImplExtra {
 // compiled into it, so its registers and code size are those of the plain solve)
 template <bool EXTRA>
 __global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, ImplArgs a, ImplExtra x) {
+  const double dt = s.coef[a.dt_slot];
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
   if (!range_cell(r, ix, iy, iz)) return;
@@ -875,20 +879,20 @@ __global__ void __launch_bounds__(128) k_implicit(DevState s, DevScalars* sc, Im
     long nd = (long)s.gr.nx * s.gr.ny * s.gr.nz, td = ix + s.gr.nx * (iy + s.gr.ny * iz);
     double g0[NV];
     for (int i = 0; i < NV; ++i) g0[i] = x.guess[i * nd + td];
-    res = solve_implicit_lab_from(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip, g0);
+    res = solve_implicit_lab_from(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, g0);
     if (!res.ok) {
       atomicAdd(x.n_fallback, 1ULL);
-      res = solve_implicit_lab(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip);
+      res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
     }
   } else {
-    res = solve_implicit_lab(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip);
+    res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
   }
   if (EXTRA && x.hx && res.ok && res.rung == 0) {
     unsigned long long k = atomicAdd(x.hcount, 1ULL);
     if ((long)k < x.hcap) {
       double ehat = -calc_ff_rtt(pp00, g, nullptr);
       int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
-      mlp_features_raw(pp00, a.dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
+      mlp_features_raw(pp00, dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
       mlp_targets_raw(pp00, pp, sw, x.ht + k * MLP_OUT);
     }
   }
@@ -919,6 +923,7 @@ struct SplitList {
   long cap;
 };
 __global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* sc, ImplArgs a, SplitList L) {
+  const double dt = s.coef[a.dt_slot];
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
   if (!range_cell(r, ix, iy, iz)) return;
@@ -930,8 +935,8 @@ __global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* s
   Geom g;
   geom_cell(s, ix, iy, iz, g);
   ImplicitPre pre;
-  implicit_prepare(pp, g, a.dt, a.gam, a.op, a.ip, pre);
-  if (implicit_first_exit(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip, pre)) {
+  implicit_prepare(pp, g, dt, a.gam, a.op, a.ip, pre);
+  if (implicit_first_exit(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, pre)) {
     store_cell(s.u, nc, c, uu);
     store_cell(s.p, nc, c, pp);
     s.flags[5 * nc + c] = 0;
@@ -948,6 +953,7 @@ __global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* s
   for (int i = 0; i < NV; ++i) L.pp0[(long)i * L.cap + (long)k] = pre.pp0[i];
 }
 __global__ void __launch_bounds__(128) k_implicit_ladder(DevState s, DevScalars* sc, ImplArgs a, SplitList L) {
+  const double dt = s.coef[a.dt_slot];
   long n = (long)*L.count;
   if (n > L.cap) n = L.cap;
   for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
@@ -966,7 +972,7 @@ __global__ void __launch_bounds__(128) k_implicit_ladder(DevState s, DevScalars*
     fill_rad_state(pp, g, a.gam, a.op, true, pre.state00);
     for (int i = 0; i < NV; ++i) pre.pp0[i] = L.pp0[(long)i * L.cap + k];
     pre.startwith = (ehat < a.ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
-    ImplicitResult res = implicit_ladder(uu, pp, g, a.dt, a.gam, a.rp, a.op, a.ip, pre);
+    ImplicitResult res = implicit_ladder(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, pre);
     if (res.ok) {
       store_cell(s.u, nc, c, uu);
       store_cell(s.p, nc, c, pp);
@@ -984,6 +990,7 @@ __global__ void __launch_bounds__(128) k_implicit_ladder(DevState s, DevScalars*
 // standardised, through the tensor-core network (one warp per 32 cells), and
 // the seeded starting state written to guess [NV][nx ny nz].
 __global__ void __launch_bounds__(128) k_mlp_guess(DevState s, MlpDev m, ImplArgs a, double* guess) {
+  const double dt = s.coef[a.dt_slot];
   __shared__ float xs[4][32 * MLP_IN];
   __shared__ float ys[4][32 * MLP_OUT];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1002,7 +1009,7 @@ __global__ void __launch_bounds__(128) k_mlp_guess(DevState s, MlpDev m, ImplArg
     geom_cell(s, ix, iy, iz, g);
     double ehat = -calc_ff_rtt(pp, g, nullptr);
     sw = (ehat < a.ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
-    mlp_features_raw(pp, a.dt, g.gdet, g.alpha, sw, f);
+    mlp_features_raw(pp, dt, g.gdet, g.alpha, sw, f);
     for (int k = 0; k < MLP_IN; ++k) f[k] = mlp_clip((f[k] - m.blob[MLP_OFF_IMEAN + k]) / m.blob[MLP_OFF_ISTD + k]);
   }
   for (int k = 0; k < MLP_IN; ++k) xs[warp][lane * MLP_IN + k] = f[k];
@@ -1031,18 +1038,21 @@ __global__ void __launch_bounds__(128) k_mlp_forward(MlpDev m, long n, const flo
 
 // the same operator as a persistent, lane-refilling state machine (bit-identical)
 __global__ void __launch_bounds__(128) k_implicit_persistent(DevState s, DevScalars* sc, ImplArgs a, long nwork) {
+  const double dt = s.coef[a.dt_slot];
   long nyb = s.gr.ny - 2L * a.polar_nc;
-  ImpStepSrc src{s, sc, a.dt, s.gr.nx, nyb, (long)a.polar_nc};
+  ImpStepSrc src{s, sc, dt, s.gr.nx, nyb, (long)a.polar_nc};
   ImpParams P{a.gam, a.rp, a.op, a.ip};
   imp_persistent(src, nwork, &sc->work_next, P);
 }
 
 // ---- radiative viscosity (koral/sim/rijvisc.zig:266) ---------------------------
 struct ViscArgs {
-  double gam, dt, rhor, alpha;
+  double gam, rhor, alpha;
+  int dt_slot;
   OpacParams op;
 };
 __global__ void __launch_bounds__(128) k_rijvisc(DevState s, ViscArgs a) {
+  const double dt = s.coef[a.dt_slot];
   long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
   Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};
   long ix, iy, iz;
@@ -1124,7 +1134,7 @@ __global__ void __launch_bounds__(128) k_rijvisc(DevState s, ViscArgs a) {
   else if (nz == 1) mindx = kmath::fmin(dx[0], dx[1]);
   else if (ny == 1) mindx = kmath::fmin(dx[0], dx[2]);
   else mindx = kmath::fmin(dx[0], kmath::fmin(dx[1], dx[2]));
-  double nu = visc_coeff(chi, mindx, s.blg[26L * nc + c], a.rhor, a.alpha, a.dt);
+  double nu = visc_coeff(chi, mindx, s.blg[26L * nc + c], a.rhor, a.alpha, dt);
   double rv[4][4];
   rij_visc(nu, pp[EE], shear, geo, rv);
   for (int i = 0; i < 4; ++i)
@@ -1172,10 +1182,12 @@ __global__ void __launch_bounds__(256) k_scale_height(DevState s) {
   if (warp == 0 && okx) s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
 }
 struct DynArgs {
-  double gam, dt, a, rhor, risco;
+  double gam, a, rhor, risco;
+  int dt_slot;
   DynamoParams dp;
 };
 __global__ void __launch_bounds__(128) k_dynamo_delta_a(DevState s, DevScalars* sc, DynArgs a) {
+  const double dt = s.coef[a.dt_slot];
   long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
   Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};
   long ix, iy, iz;
@@ -1202,7 +1214,7 @@ __global__ void __launch_bounds__(128) k_dynamo_delta_a(DevState s, DevScalars* 
   double ehat = -calc_ff_rtt(pp, geo, nullptr);
   prermhd += ehat / 3.0;
   long gix = ix < 0 ? 0 : (ix > s.gr.nx - 1 ? s.gr.nx - 1 : ix);
-  DynamoOut o = dynamo_delta_a(a.dp, a.a, a.dt, a.rhor, a.risco, rr, th, pp[B3], bsq, angle, prermhd, geo.gg[3][3],
+  DynamoOut o = dynamo_delta_a(a.dp, a.a, dt, a.rhor, a.risco, rr, th, pp[B3], bsq, angle, prermhd, geo.gg[3][3],
                                s.scaleth[gix]);
   s.dyn_a[c] = o.aphi;
   if (a.dp.dampbeta) s.p[B3 * nc + c] = o.bphi;

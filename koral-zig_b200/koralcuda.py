@@ -79,6 +79,12 @@ class KcCounters(ctypes.Structure):
                 ("n_radimp_solves", ctypes.c_int64), ("n_guard_recoveries", ctypes.c_int64)]
 
 
+class KcTuneResult(ctypes.Structure):
+    _fields_ = [("implicit_mode", ctypes.c_int32), ("tpb_implicit", ctypes.c_int32), ("tpb_flux", ctypes.c_int32),
+                ("tpb_u2p", ctypes.c_int32), ("ms_per_step", _d), ("ms_per_step_entry", _d),
+                ("trials", ctypes.c_int32)]
+
+
 class KcStepInfo(ctypes.Structure):
     _fields_ = [("dt", _d), ("nan_cell", ctypes.c_int64)]
 
@@ -117,6 +123,8 @@ def lib():
     L.kc_step_n.argtypes = [vp, i32, dbl]
     L.kc_set_precision.argtypes = [vp, i32]
     L.kc_set_implicit_mode.argtypes = [vp, i32]
+    L.kc_set_graph.argtypes = [vp, i32]
+    L.kc_autotune.argtypes = [vp, i32, P(KcTuneResult)]
     L.kc_set_guess.argtypes = [vp, i32, vp, i64]
     L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64, P(dbl)]
     L.kc_implicit_batch.argtypes = [P(KcOptions), i64, vp, vp, vp, vp, i32]
@@ -138,6 +146,7 @@ def lib():
     L.kc_mlp_train.argtypes = [vp, vp, i64, i32, i32, ctypes.c_float, ctypes.c_uint64, vp, vp]
     L.kc_mlp_forward.argtypes = [vp, i64, vp, vp]
     L.kc_mlp_grad.argtypes = [vp, i64, vp, vp, vp, vp]
+    L.kc_fp64_peak.argtypes = [P(dbl)]
     L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
     L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
     for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
@@ -147,7 +156,7 @@ def lib():
               "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
               "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc", "kc_implicit_batch_device",
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
-              "kc_mlp_forward", "kc_mlp_grad"]:
+              "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -275,6 +284,17 @@ class Sim:
         dt = float("nan") if forced_dt is None else float(forced_dt)
         self._check(self._lib.kc_step(self._h, dt, ctypes.byref(info)))
         return info.dt
+
+    def set_graph(self, on):
+        """Capture the step as a CUDA graph and replay it (bit-identical)."""
+        self._check(self._lib.kc_set_graph(self._h, 1 if on else 0))
+
+    def autotune(self, steps=2):
+        """kc_autotune: pick the implicit form and block sizes by timing steps on
+        the current state (restored afterwards); returns the choice."""
+        r = KcTuneResult()
+        self._check(self._lib.kc_autotune(self._h, steps, ctypes.byref(r)))
+        return {k: getattr(r, k) for k, _ in KcTuneResult._fields_}
 
     def set_precision(self, mode):
         """KC_PLAIN_FP64 or KC_MIXED (FP32 reconstruction, LAXF and flux-CT)."""
@@ -439,3 +459,10 @@ def mlp_grad(weights, features_std, targets_std):
     _status(lib().kc_mlp_grad(w.ctypes.data, x.shape[0], x.ctypes.data, t.ctypes.data, g.ctypes.data,
                               ctypes.byref(loss)), "kc_mlp_grad")
     return float(loss.value), g
+
+
+def fp64_peak():
+    """Measured FP64 (DFMA) peak of the current device in TFLOP/s."""
+    v = ctypes.c_double(0.0)
+    _status(lib().kc_fp64_peak(ctypes.byref(v)), "kc_fp64_peak")
+    return v.value

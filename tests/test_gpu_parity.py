@@ -199,3 +199,58 @@ def test_scalar_row_bitwise_vs_oracle_3d():
     gpu.step()
     orc.step()
     _scalars_equal(gpu.scalars(0.0, 40.0, 15.0), orc.scalar_row(0.0, 40.0, 15.0))
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_graph_replay_matches_oracle(mode):
+    """The step as a captured CUDA graph (kc_set_graph): the first step runs
+    eagerly, the second is captured, the rest replay it with each step's own dt
+    (CFL and forced); every state matches the oracle bit for bit, and a change
+    of form mid-run re-captures."""
+    kc = _kc()
+    grid, opt = kc.puffy_grid(24, 20, 8), kc.puffy_options(implicit_mode=mode)
+    gpu, orc = _pair(grid, opt)
+    assert gpu.initPuffy(1e-3, 1e-3, 777) == orc.init_puffy(1e-3, 1e-3, 777)
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    gpu.set_graph(True)
+    n0 = gpu.launch_count()
+    for k in range(5):
+        forced = None if k != 3 else 0.8 * orc.counters()["dt"]
+        gpu.step(forced)
+        orc.step(float("nan") if forced is None else forced)
+        _assert_same_state(gpu, orc)
+    per_step = (gpu.launch_count() - n0) / 5
+    assert per_step == int(per_step) and per_step > 50
+    cg, co = gpu.counters(), orc.counters()
+    for k in ["t", "dt", "tstepdenmax", "tstepdenmin", "n_radimp_failures", "n_radimp_iters", "n_radimp_solves"]:
+        assert cg[k] == co[k], (k, cg[k], co[k])
+    other = 1 if mode != 1 else 0
+    assert kc.lib().kc_set_implicit_mode(gpu._h, other) == 0
+    for _ in range(3):
+        gpu.step()
+        orc.step()
+        _assert_same_state(gpu, orc)
+
+
+def test_autotune_restores_state_and_keeps_bits():
+    """kc_autotune times candidates from a snapshot, restores the state and the
+    counters, and leaves a configuration whose steps are bit-identical to the
+    default one's."""
+    kc = _kc()
+    grid = kc.puffy_grid(48, 40, 8)
+    a, b = kc.Sim(grid, kc.puffy_options()), kc.Sim(grid, kc.puffy_options())
+    for s in (a, b):
+        s.initPuffy(1e-3, 1e-3, 99)
+        s.step()
+    p0, c0 = b.p, b.counters()
+    r = b.autotune(1)
+    assert r["implicit_mode"] in (0, 2) and r["trials"] >= 2
+    for k in ("tpb_implicit", "tpb_flux", "tpb_u2p"):
+        assert r[k] in (64, 96, 128)
+    assert np.array_equal(b.p, p0) and b.counters() == c0
+    b.set_graph(True)
+    for _ in range(3):
+        a.step()
+        b.step()
+    assert np.array_equal(a.p, b.p) and np.array_equal(a.u, b.u) and np.array_equal(a.flags, b.flags)
+    assert a.counters() == b.counters()

@@ -39,7 +39,13 @@ enum {
   KC_ERR_CUDA = 6,
   KC_ERR_TIMEOUT = 7,
   KC_ERR_NO_DEVICE = 8,
-  KC_ERR_TOO_MANY_CELLS = 9 /* more cells than kc_implicit_batch_noalloc stages */
+  KC_ERR_TOO_MANY_CELLS = 9, /* more cells than kc_implicit_batch_noalloc stages */
+  /* dump.zig:41 ReadError of the KDMP reader */
+  KC_ERR_KDMP_BAD_MAGIC = 10,
+  KC_ERR_KDMP_BAD_VERSION = 11,
+  KC_ERR_KDMP_DIM_MISMATCH = 12,
+  KC_ERR_KDMP_TRUNCATED = 13,
+  KC_ERR_IO = 14 /* a KDMP file could not be opened, read or written */
 };
 
 enum { KC_BC_PERIODIC = 0, KC_BC_COPY = 1, KC_BC_PUFFY = 2 };
@@ -293,6 +299,37 @@ int kc_mlp_train(const float* features, const float* targets, int64_t n, int32_t
 int kc_mlp_forward(const float* weights, int64_t n, const float* features_std, float* out_std);
 int kc_mlp_grad(const float* weights, int64_t n, const float* features_std, const float* targets_std, float* grad,
                 float* loss);
+
+/* KDMP v2 checkpoints (koral/io/dump.zig): a 44-byte little-endian header
+ * (magic "KDMP", version 2, nx ny nz nv as u32, t f64, nstep u64, out_idx u32;
+ * dump.zig:29 DumpHeader, :38 header_size) followed by the domain primitives
+ * p[nz][ny][nx][nv] as f64, iv fastest (dump.zig:100 serializePrimDump). */
+#define KC_KDMP_HEADER_SIZE 44
+#define KC_KDMP_VERSION 2
+typedef struct kc_dump_header {
+  uint32_t nx, ny, nz, nv;
+  double t;
+  uint64_t nstep;
+  uint32_t out_idx;
+} kc_dump_header;
+/* writeDumpHeader (dump.zig:67) into out[KC_KDMP_HEADER_SIZE]; host only */
+int kc_kdmp_write_header(const kc_dump_header* hd, uint8_t* out);
+/* parseDumpHeader (dump.zig:86): magic, version and length checked; host only */
+int kc_kdmp_parse_header(const uint8_t* bytes, int64_t len, kc_dump_header* hd);
+/* primDumpSize (dump.zig:45) of the handle's grid */
+int64_t kc_kdmp_size(kc_handle* h);
+/* serializePrimDump (dump.zig:100) of the device state: the domain is gathered
+ * into AoS order on the device and copied out once; t and nstep from the
+ * handle. `capacity` must be at least kc_kdmp_size. */
+int kc_kdmp_write(kc_handle* h, uint32_t out_idx, uint8_t* out, int64_t capacity, int64_t* written);
+/* loadPrimDump (dump.zig:143): header checks (dims against the handle's grid),
+ * then per domain cell p = the stored primitives and u = p2u(p) on the device,
+ * as Sim.initCell (koral/sim.zig:672) does. As in the reference, the caller
+ * adopts t / nstep from *hd (kc_set_counters) and runs kc_finish_init. */
+int kc_kdmp_load(kc_handle* h, const uint8_t* bytes, int64_t len, kc_dump_header* hd);
+/* writePrim / loadPrim (dump.zig:213, :270), serial: the same through a file */
+int kc_kdmp_write_file(kc_handle* h, const char* path, uint32_t out_idx);
+int kc_kdmp_load_file(kc_handle* h, const char* path, kc_dump_header* hd);
 
 /* The FP64 pipe's peak on the current device, measured: independent DFMA
  * chains over every SM, best of five launches, in TFLOP/s (the denominator of

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "kc_kernels.cuh"
+#include "../../include/koral/kdump.h"
 #include "../../include/koral/kinit.h"
 
 using namespace kp;
@@ -111,6 +112,14 @@ struct kc_handle {
 
 namespace {
 
+// A rejected argument (unknown mode, bad file, short buffer): the message is
+// kept for kc_last_error, but the handle stays usable.
+int reject(kc_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+// A failure of the device state (a CUDA error, a failed pass): every later
+// step call returns it.
 int fail(kc_handle* h, int code, const std::string& msg) {
   if (h) {
     h->err = msg;
@@ -1089,7 +1098,7 @@ int kc_step_n(kc_handle* h, int32_t nsteps, double forced_dt) {
 // debugging surface for the parity tests: run one pass
 int kc_set_pass_timing(kc_handle* h, int32_t on) {
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (h->pass_depth) return fail(h, KC_ERR_INVALID_CONFIG, "pass timing changed inside a pass");
+  if (h->pass_depth) return reject(h, KC_ERR_INVALID_CONFIG, "pass timing changed inside a pass");
   h->timing = on != 0;
   h->ev_pass.clear();
   for (int i = 0; i < KC_NPASS; ++i) {
@@ -1166,7 +1175,7 @@ int kc_debug_get_array(kc_handle* h, int which, double* out) {
 
 int kc_set_precision(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (mode != KC_PLAIN_FP64 && mode != KC_MIXED) return fail(h, KC_ERR_INVALID_CONFIG, "unknown precision mode");
+  if (mode != KC_PLAIN_FP64 && mode != KC_MIXED) return reject(h, KC_ERR_INVALID_CONFIG, "unknown precision mode");
   h->opt.precision = mode;
   drop_graph(h);
   return KC_OK;
@@ -1174,7 +1183,7 @@ int kc_set_precision(kc_handle* h, int32_t mode) {
 int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING && mode != KC_IMPLICIT_SPLIT)
-    return fail(h, KC_ERR_INVALID_CONFIG, "unknown implicit mode");
+    return reject(h, KC_ERR_INVALID_CONFIG, "unknown implicit mode");
   h->opt.implicit_mode = mode;
   drop_graph(h);
   return KC_OK;
@@ -1200,13 +1209,13 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
     drop_graph(h);
     return KC_OK;
   }
-  if (mode != KC_GUESS_MLP) return fail(h, KC_ERR_INVALID_CONFIG, "unknown guess mode");
+  if (mode != KC_GUESS_MLP) return reject(h, KC_ERR_INVALID_CONFIG, "unknown guess mode");
   if (!weights || nweights != KC_MLP_NWEIGHTS)
-    return fail(h, KC_ERR_INVALID_CONFIG, "learned guess needs KC_MLP_NWEIGHTS floats");
+    return reject(h, KC_ERR_INVALID_CONFIG, "learned guess needs KC_MLP_NWEIGHTS floats");
   for (int64_t i = 0; i < nweights; ++i)
-    if (!std::isfinite(weights[i])) return fail(h, KC_ERR_INVALID_CONFIG, "non-finite guess weight");
+    if (!std::isfinite(weights[i])) return reject(h, KC_ERR_INVALID_CONFIG, "non-finite guess weight");
   for (int k = 0; k < MLP_IN; ++k)
-    if (!(weights[MLP_OFF_ISTD + k] > 0.0f)) return fail(h, KC_ERR_INVALID_CONFIG, "guess input std must be > 0");
+    if (!(weights[MLP_OFF_ISTD + k] > 0.0f)) return reject(h, KC_ERR_INVALID_CONFIG, "guess input std must be > 0");
   int st = ensure_imp_ctr(h);
   const DGrid& gr = h->gr;
   long ndom = (long)gr.nx * gr.ny * gr.nz;
@@ -1965,8 +1974,8 @@ extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
   if (!h || steps < 1) return KC_ERR_INVALID_CONFIG;
   if (h->last_status) return h->last_status;
   if (h->guess_mode != KC_GUESS_PLAIN || h->hcap > 0)
-    return fail(h, KC_ERR_INVALID_CONFIG, "autotune with the learned guess or the harvest on");
-  if (h->timing) return fail(h, KC_ERR_INVALID_CONFIG, "autotune with pass timing on");
+    return reject(h, KC_ERR_INVALID_CONFIG, "autotune with the learned guess or the harvest on");
+  if (h->timing) return reject(h, KC_ERR_INVALID_CONFIG, "autotune with pass timing on");
   int st = cuda_check(h, cudaStreamSynchronize(h->stream), "autotune");
   if (st) return st;
   TuneSnapshot sn;
@@ -2041,4 +2050,83 @@ extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
     out->trials = trials;
   }
   return KC_OK;
+}
+
+// ---- KDMP v2 checkpoints (koral/io/dump.zig) ---------------------------------------
+extern "C" int kc_kdmp_write_header(const kc_dump_header* hd, uint8_t* out) {
+  if (!hd || !out) return KC_ERR_INVALID_CONFIG;
+  kdump::write_header(*hd, out);
+  return KC_OK;
+}
+extern "C" int kc_kdmp_parse_header(const uint8_t* bytes, int64_t len, kc_dump_header* hd) {
+  if (!hd) return KC_ERR_INVALID_CONFIG;
+  return kdump::parse_header(bytes, len, *hd);
+}
+extern "C" int64_t kc_kdmp_size(kc_handle* h) {
+  if (!h) return -1;
+  return KC_KDMP_HEADER_SIZE + kdump::body_bytes(h->gr.nx, h->gr.ny, h->gr.nz, NV);
+}
+extern "C" int kc_kdmp_write(kc_handle* h, uint32_t out_idx, uint8_t* out, int64_t capacity, int64_t* written) {
+  if (!h || !out) return KC_ERR_INVALID_CONFIG;
+  if (written) *written = 0;
+  int64_t need = kc_kdmp_size(h);
+  if (capacity < need) return reject(h, KC_ERR_INVALID_CONFIG, "KDMP buffer smaller than kc_kdmp_size");
+  const DGrid& gr = h->gr;
+  long nd = (long)gr.nx * gr.ny * gr.nz;
+  // the staging array holds NV x (cells incl. ghosts) doubles, more than the body
+  k_domain_to_kdmp<<<nblk(nd * NV, 256), 256, 0, h->stream>>>(h->ds, h->staging);
+  int st = cuda_check(h, cudaMemcpyAsync(out + KC_KDMP_HEADER_SIZE, h->staging, (size_t)nd * NV * 8,
+                                         cudaMemcpyDeviceToHost, h->stream), "KDMP write");
+  if (!st) st = cuda_check(h, cudaStreamSynchronize(h->stream), "KDMP write");
+  if (st) return st;
+  kc_dump_header hd = {(uint32_t)gr.nx, (uint32_t)gr.ny, (uint32_t)gr.nz, (uint32_t)NV, h->t, (uint64_t)h->nstep,
+                       out_idx};
+  kdump::write_header(hd, out);
+  if (written) *written = need;
+  return KC_OK;
+}
+extern "C" int kc_kdmp_load(kc_handle* h, const uint8_t* bytes, int64_t len, kc_dump_header* hd_out) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  kc_dump_header hd;
+  int st = kdump::parse_header(bytes, len, hd);
+  if (st) return reject(h, st, "KDMP header");
+  const DGrid& gr = h->gr;
+  if (hd.nx != (uint32_t)gr.nx || hd.ny != (uint32_t)gr.ny || hd.nz != (uint32_t)gr.nz || hd.nv != (uint32_t)NV)
+    return reject(h, KC_ERR_KDMP_DIM_MISMATCH, "KDMP grid differs from the handle's");
+  long nd = (long)gr.nx * gr.ny * gr.nz;
+  if (len < kc_kdmp_size(h)) return reject(h, KC_ERR_KDMP_TRUNCATED, "KDMP body truncated");
+  st = cuda_check(h, cudaMemcpyAsync(h->staging, bytes + KC_KDMP_HEADER_SIZE, (size_t)nd * NV * 8,
+                                     cudaMemcpyHostToDevice, h->stream), "KDMP load");
+  if (st) return st;
+  k_kdmp_to_domain<<<nblk(nd), TPB, 0, h->stream>>>(h->ds, h->staging, h->sp.gam);
+  st = cuda_check(h, cudaStreamSynchronize(h->stream), "KDMP load");
+  if (st) return st;
+  if (hd_out) *hd_out = hd;
+  return KC_OK;
+}
+extern "C" int kc_kdmp_write_file(kc_handle* h, const char* path, uint32_t out_idx) {
+  if (!h || !path) return KC_ERR_INVALID_CONFIG;
+  int64_t n = kc_kdmp_size(h);
+  std::vector<uint8_t> buf((size_t)n);
+  int st = kc_kdmp_write(h, out_idx, buf.data(), n, nullptr);
+  if (st) return st;
+  FILE* f = fopen(path, "wb");
+  if (!f) return reject(h, KC_ERR_IO, std::string("cannot create ") + path);
+  size_t w = fwrite(buf.data(), 1, buf.size(), f);
+  int c = fclose(f);
+  if (w != buf.size() || c != 0) return reject(h, KC_ERR_IO, std::string("cannot write ") + path);
+  return KC_OK;
+}
+extern "C" int kc_kdmp_load_file(kc_handle* h, const char* path, kc_dump_header* hd) {
+  if (!h || !path) return KC_ERR_INVALID_CONFIG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return reject(h, KC_ERR_IO, std::string("cannot open ") + path);
+  std::vector<uint8_t> buf;
+  uint8_t chunk[1 << 16];
+  size_t r;
+  while ((r = fread(chunk, 1, sizeof chunk, f)) > 0) buf.insert(buf.end(), chunk, chunk + r);
+  bool err = ferror(f) != 0;
+  fclose(f);
+  if (err) return reject(h, KC_ERR_IO, std::string("cannot read ") + path);
+  return kc_kdmp_load(h, buf.data(), (int64_t)buf.size(), hd);
 }

@@ -48,6 +48,33 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
   int v = (int)(t % nv);
   aos[t] = soa[(long)v * nc + c];
 }
+// KDMP body (dump.zig:122 serializePrimBody): the domain primitives in
+// [iz][iy][ix][iv] order, one thread per output double (coalesced writes)
+__global__ void k_domain_to_kdmp(DevState s, double* __restrict__ body) {
+  long nx = s.gr.nx, ny = s.gr.ny, nd = nx * ny * s.gr.nz;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nd * NV) return;
+  long d = t / NV;
+  int v = (int)(t % NV);
+  long c = cidx(s.gr, d % nx, (d / nx) % ny, d / (nx * ny));
+  body[t] = s.p[(long)v * s.gr.nc + c];
+}
+// KDMP load (dump.zig:160 loadPrimBody + sim.zig:672 initCell): p stored as
+// read, u = p2u(p) with the cell's geometry, one thread per domain cell
+__global__ void __launch_bounds__(128) k_kdmp_to_domain(DevState s, const double* __restrict__ body, double gam) {
+  long nx = s.gr.nx, ny = s.gr.ny, nd = nx * ny * s.gr.nz;
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= nd) return;
+  long ix = d % nx, iy = (d / nx) % ny, iz = d / (nx * ny);
+  long c = cidx(s.gr, ix, iy, iz);
+  double pp[NV], uu[NV];
+  for (int v = 0; v < NV; ++v) pp[v] = body[d * NV + v];
+  Geom g;
+  geom_cell(s, ix, iy, iz, g);
+  p2u(pp, uu, g, gam);
+  store_cell(s.p, s.gr.nc, c, pp);
+  store_cell(s.u, s.gr.nc, c, uu);
+}
 __global__ void k_flags_to_soa(const int* __restrict__ aos, int* __restrict__ soa, long nc) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nc * 6) return;

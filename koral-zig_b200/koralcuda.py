@@ -27,6 +27,8 @@ KC_NPASS = 14
 KC_ERR_TOO_MANY_CELLS = 9
 KC_NOALLOC_MAX_CELLS = 16384
 KC_GUESS_PLAIN, KC_GUESS_MLP = 0, 1
+KC_ERR_KDMP_BAD_MAGIC, KC_ERR_KDMP_BAD_VERSION, KC_ERR_KDMP_DIM_MISMATCH, KC_ERR_KDMP_TRUNCATED, KC_ERR_IO = 10, 11, 12, 13, 14
+KC_KDMP_HEADER_SIZE = 44
 KC_MLP_IN, KC_MLP_HIDDEN, KC_MLP_OUT, KC_MLP_NWEIGHTS = 16, 64, 4, 5548
 
 
@@ -77,6 +79,11 @@ class KcCounters(ctypes.Structure):
                 ("nstep", ctypes.c_int64), ("n_radimp_failures", ctypes.c_int64),
                 ("n_radimp_fail_step", ctypes.c_int64), ("n_radimp_iters", ctypes.c_int64),
                 ("n_radimp_solves", ctypes.c_int64), ("n_guard_recoveries", ctypes.c_int64)]
+
+
+class KcDumpHeader(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_uint32), ("ny", ctypes.c_uint32), ("nz", ctypes.c_uint32), ("nv", ctypes.c_uint32),
+                ("t", _d), ("nstep", ctypes.c_uint64), ("out_idx", ctypes.c_uint32)]
 
 
 class KcTuneResult(ctypes.Structure):
@@ -147,6 +154,14 @@ def lib():
     L.kc_mlp_forward.argtypes = [vp, i64, vp, vp]
     L.kc_mlp_grad.argtypes = [vp, i64, vp, vp, vp, vp]
     L.kc_fp64_peak.argtypes = [P(dbl)]
+    L.kc_kdmp_write_header.argtypes = [P(KcDumpHeader), vp]
+    L.kc_kdmp_parse_header.argtypes = [vp, i64, P(KcDumpHeader)]
+    L.kc_kdmp_size.argtypes = [vp]
+    L.kc_kdmp_size.restype = i64
+    L.kc_kdmp_write.argtypes = [vp, ctypes.c_uint32, vp, i64, P(i64)]
+    L.kc_kdmp_load.argtypes = [vp, vp, i64, P(KcDumpHeader)]
+    L.kc_kdmp_write_file.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint32]
+    L.kc_kdmp_load_file.argtypes = [vp, ctypes.c_char_p, P(KcDumpHeader)]
     L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
     L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
     for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
@@ -156,7 +171,9 @@ def lib():
               "kc_u2p_batch", "kc_debug_phase", "kc_debug_get_array", "kc_set_pass_timing", "kc_get_pass_times",
               "kc_get_stream", "kc_get_launch_count", "kc_implicit_batch_noalloc", "kc_implicit_batch_device",
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
-              "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune"]:
+              "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune",
+              "kc_kdmp_write_header", "kc_kdmp_parse_header", "kc_kdmp_write", "kc_kdmp_load", "kc_kdmp_write_file",
+              "kc_kdmp_load_file"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -360,6 +377,30 @@ class Sim:
     def guess_fallbacks(self):
         return int(self._lib.kc_guess_fallbacks(self._h))
 
+    # ---- KDMP v2 checkpoints (koral/io/dump.zig) ---------------------------------
+    def kdmp_write(self, out_idx=0):
+        """serializePrimDump of the device state: the KDMP file bytes."""
+        n = self._lib.kc_kdmp_size(self._h)
+        buf = (ctypes.c_uint8 * n)()
+        w = ctypes.c_int64(0)
+        self._check(self._lib.kc_kdmp_write(self._h, out_idx, buf, n, ctypes.byref(w)))
+        return bytes(buf)[:w.value]
+
+    def kdmp_load(self, data):
+        """loadPrimDump: p from the file, u = p2u(p); returns the header (the
+        caller adopts t / nstep and runs finishInit, as in the reference)."""
+        hd = KcDumpHeader()
+        self._check(self._lib.kc_kdmp_load(self._h, data, len(data), ctypes.byref(hd)))
+        return {k: getattr(hd, k) for k, _ in KcDumpHeader._fields_}
+
+    def kdmp_write_file(self, path, out_idx=0):
+        self._check(self._lib.kc_kdmp_write_file(self._h, os.fsencode(path), out_idx))
+
+    def kdmp_load_file(self, path):
+        hd = KcDumpHeader()
+        self._check(self._lib.kc_kdmp_load_file(self._h, os.fsencode(path), ctypes.byref(hd)))
+        return {k: getattr(hd, k) for k, _ in KcDumpHeader._fields_}
+
     def debug_phase(self, phase, dt=0.0):
         self._check(self._lib.kc_debug_phase(self._h, phase, dt))
 
@@ -466,3 +507,19 @@ def fp64_peak():
     v = ctypes.c_double(0.0)
     _status(lib().kc_fp64_peak(ctypes.byref(v)), "kc_fp64_peak")
     return v.value
+
+
+def kdmp_write_header(nx, ny, nz, nv, t, nstep, out_idx):
+    """writeDumpHeader (koral/io/dump.zig:67): the 44 header bytes (host only)."""
+    hd = KcDumpHeader(nx, ny, nz, nv, t, nstep, out_idx)
+    buf = (ctypes.c_uint8 * KC_KDMP_HEADER_SIZE)()
+    _status(lib().kc_kdmp_write_header(ctypes.byref(hd), buf), "kc_kdmp_write_header")
+    return bytes(buf)
+
+
+def kdmp_parse_header(data):
+    """parseDumpHeader (koral/io/dump.zig:86); raises KoralError with the
+    reader's status (BadMagic 10, BadVersion 11, Truncated 13)."""
+    hd = KcDumpHeader()
+    _status(lib().kc_kdmp_parse_header(data, len(data), ctypes.byref(hd)), "kc_kdmp_parse_header")
+    return {k: getattr(hd, k) for k, _ in KcDumpHeader._fields_}

@@ -21,6 +21,7 @@
 #include <thread>
 #include <vector>
 
+#include "../include/koral/kdump.h"
 #include "../include/koral/kinit.h"
 #include "../include/koral/kvisc.h"
 
@@ -1801,6 +1802,51 @@ int orc_sim_phase(void* h, int phase, double dt) {
     case 9: return op_explicit(s, dt);
     default: return -1;
   }
+}
+// KDMP v2 (dump.zig:100 serializePrimDump, :143 loadPrimDump): serial loops
+// over the domain, iz slowest, iv fastest; the load stores p verbatim and u =
+// p2u(p) per cell (sim.zig:672 initCell). The caller adopts t / nstep.
+long orc_sim_kdmp_size(void* h) {
+  OSim& s = *(OSim*)h;
+  return KC_KDMP_HEADER_SIZE + kdump::body_bytes(s.g.nx, s.g.ny, s.g.nz, NV);
+}
+int orc_sim_kdmp_write(void* h, unsigned out_idx, unsigned char* out, long cap) {
+  OSim& s = *(OSim*)h;
+  if (cap < orc_sim_kdmp_size(h)) return KC_ERR_INVALID_CONFIG;
+  kc_dump_header hd = {(uint32_t)s.g.nx, (uint32_t)s.g.ny, (uint32_t)s.g.nz, (uint32_t)NV, s.t, (uint64_t)s.nstep,
+                       out_idx};
+  long w = kdump::write_header(hd, out);
+  for (long iz = 0; iz < s.g.nz; ++iz)
+    for (long iy = 0; iy < s.g.ny; ++iy)
+      for (long ix = 0; ix < s.g.nx; ++ix)
+        for (int iv = 0; iv < NV; ++iv) {
+          memcpy(out + w, &s.P(ix, iy, iz)[iv], 8);
+          w += 8;
+        }
+  return KC_OK;
+}
+int orc_sim_kdmp_load(void* h, const unsigned char* b, long len, kc_dump_header* out) {
+  OSim& s = *(OSim*)h;
+  kc_dump_header hd;
+  int st = kdump::parse_header(b, len, hd);
+  if (st) return st;
+  if (hd.nx != (uint32_t)s.g.nx || hd.ny != (uint32_t)s.g.ny || hd.nz != (uint32_t)s.g.nz || hd.nv != (uint32_t)NV)
+    return KC_ERR_KDMP_DIM_MISMATCH;
+  if (len < orc_sim_kdmp_size(h)) return KC_ERR_KDMP_TRUNCATED;
+  long r = KC_KDMP_HEADER_SIZE;
+  for (long iz = 0; iz < s.g.nz; ++iz)
+    for (long iy = 0; iy < s.g.ny; ++iy)
+      for (long ix = 0; ix < s.g.nx; ++ix) {
+        double pp[NV];
+        for (int iv = 0; iv < NV; ++iv) {
+          memcpy(&pp[iv], b + r, 8);
+          r += 8;
+        }
+        for (int iv = 0; iv < NV; ++iv) s.P(ix, iy, iz)[iv] = pp[iv];
+        p2u_cell(s, ix, iy, iz);
+      }
+  if (out) *out = hd;
+  return KC_OK;
 }
 // read-only views of internal arrays for parity tests
 int orc_sim_get_array(void* h, int which, double* out) {

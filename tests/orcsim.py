@@ -59,6 +59,12 @@ def _bind():
     lib.orc_sim_scalar_row.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                        ctypes.POINTER(KcScalarRow)]
     lib.orc_sim_scalar_row.restype = ctypes.c_int
+    lib.orc_sim_kdmp_size.argtypes = [vp]
+    lib.orc_sim_kdmp_size.restype = ctypes.c_long
+    lib.orc_sim_kdmp_write.argtypes = [vp, ctypes.c_uint, vp, ctypes.c_long]
+    lib.orc_sim_kdmp_write.restype = ctypes.c_int
+    lib.orc_sim_kdmp_load.argtypes = [vp, vp, ctypes.c_long, ctypes.POINTER(_kc.KcDumpHeader)]
+    lib.orc_sim_kdmp_load.restype = ctypes.c_int
     lib.orc_options_puffy.argtypes = [ctypes.POINTER(KcOptions)]
     lib.orc_grid_puffy.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(KcGrid)]
     _sim_bound = True
@@ -132,6 +138,21 @@ class OracleSim:
         c = KcCounters()
         self.lib.orc_sim_get_counters(self.h, ctypes.byref(c))
         return {k: getattr(c, k) for k, _ in KcCounters._fields_}
+
+    def kdmp_write(self, out_idx=0):
+        """serializePrimDump (koral/io/dump.zig:100) of the oracle state."""
+        n = self.lib.orc_sim_kdmp_size(self.h)
+        buf = (ctypes.c_uint8 * n)()
+        rc = self.lib.orc_sim_kdmp_write(self.h, out_idx, buf, n)
+        if rc:
+            raise RuntimeError(f"oracle KDMP write failed with status {rc}")
+        return bytes(buf)
+
+    def kdmp_load(self, data):
+        """loadPrimDump (koral/io/dump.zig:143); returns (status, header dict)."""
+        hd = _kc.KcDumpHeader()
+        rc = self.lib.orc_sim_kdmp_load(self.h, data, len(data), ctypes.byref(hd))
+        return rc, {k: getattr(hd, k) for k, _ in _kc.KcDumpHeader._fields_}
 
     def step(self, forced_dt=float("nan")):
         rc = self.lib.orc_sim_step(self.h, forced_dt)

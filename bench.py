@@ -523,7 +523,9 @@ def main():
     kc = load_engine()
     grid = kc.puffy_grid(args.nx, args.ny, args.nz)
     opt = kc.puffy_options(device=local, implicit_mode=IMPLICIT_MODES[args.implicit_mode])
+    t0 = time.perf_counter()
     sim = kc.Sim(grid, opt)
+    create_s = time.perf_counter() - t0
     ncell = args.nx * args.ny * args.nz
     ndim = sum(1 for d in (args.nx, args.ny, args.nz) if d > 1)
     t0 = time.perf_counter()
@@ -652,7 +654,7 @@ def main():
         "dtype": "f64", "data": "synthetic (PUFFY torus from the engine's init + seeded 1e-3 rho/u_int noise)",
         "config": {"workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz} MKS2 (periodic phi), plain FP64",
                    "cells": ncell, "ghosts": 3, "precision": "plain FP64", "l2": "inputs larger than L2 (no flush)",
-                   "init_seconds": init_s, "beta_norm_factor": fac, "parallelism": f"replicas x{world}",
+                   "create_seconds": create_s, "init_seconds": init_s, "beta_norm_factor": fac, "parallelism": f"replicas x{world}",
                    "implicit_mode": args.implicit_mode if tune is None else
                    {0: "per-cell", 1: "compacting", 2: "split"}[tune["implicit_mode"]],
                    "cuda_graph": bool(args.graph), "autotune": tune,

@@ -4,7 +4,10 @@
 // Restates koral/problems/puffy/puffy.zig:316-819 and the GK21 quadrature of
 // koral/math/quad.zig (QUADPACK dqk21 nodes and weights). The per-(x1,x2)
 // profile is computed once and replicated over the phi cells: the metric is
-// axisymmetric, so every phi cell of a column gets the same bits.
+// axisymmetric, so every phi cell of a column gets the same bits. Everything
+// here is host-and-device code (KC_HDI): the oracle runs it on the host, the
+// engine runs the torus solve one thread per column and the per-cell
+// preparation one thread per cell on the device.
 #pragma once
 #include <stdint.h>
 
@@ -25,14 +28,14 @@ struct PuffyPhysics {
   double mass = 10.0;
 };
 
-const double kXacc = 5.0 * 2.220446049250313e-16;  // 5 DBL_EPSILON
-const double kPi2 = KP_PI / 2.0;
+constexpr double kXacc = 5.0 * 2.220446049250313e-16;  // 5 DBL_EPSILON
+constexpr double kPi2 = KP_PI / 2.0;
 
 struct Gd {
   double gdtt, gdtp, gdpp;
 };
 // tools.c compute_gd (puffy.zig:345)
-inline Gd compute_gd(double r, double th, double a) {
+KC_HDI Gd compute_gd(double r, double th, double a) {
   double ac = a * kmath::cos(th);
   double sigma = ac * ac + r * r;
   double s2 = kmath::sin(th) * kmath::sin(th);
@@ -44,18 +47,18 @@ inline Gd compute_gd(double r, double th, double a) {
   return g;
 }
 // puffy.zig:358 lK
-inline double lK(double r, double a) {
+KC_HDI double lK(double r, double a) {
   double curly_f = 1.0 - 2.0 * a / kmath::pow(r, 1.5) + (a / r) * (a / r);
   double curly_g = 1.0 - 2.0 / r + a / kmath::pow(r, 1.5);
   return kmath::sqrt(r) * curly_f / curly_g;
 }
-inline double l3d(double lam, double a, double lb1, double lb2, double xi) {
+KC_HDI double l3d(double lam, double a, double lb1, double lb2, double xi) {
   double arg = lam <= lb1 ? lb1 : (lam >= lb2 ? lb2 : lam);
   return xi * lK(arg, a);
 }
 // HARM rtbis (puffy.zig:374)
 template <class F>
-double rtbis(const F& func, double x1, double x2, double xacc) {
+KC_HDI double rtbis(const F& func, double x1, double x2, double xacc) {
   double f = func(x1);
   double fmid = func(x2);
   (void)fmid;
@@ -76,18 +79,18 @@ double rtbis(const F& func, double x1, double x2, double xacc) {
   }
   return 0.0;
 }
-inline double lam_bl(double R, const Gd& gd, double a, double lb1, double lb2, double xi) {
+KC_HDI double lam_bl(double R, const Gd& gd, double a, double lb1, double lb2, double xi) {
   auto f = [&](double lam) {
     double l = l3d(lam, a, lb1, lb2, xi);
     return lam * lam + l * (l * gd.gdtp + gd.gdpp) / (l * gd.gdtt + gd.gdtp);
   };
   return rtbis(f, R, 10.0 * R, kXacc);
 }
-inline double omega3d(double l, const Gd& gd) { return -(gd.gdtt * l + gd.gdtp) * (1.0 / (gd.gdpp + gd.gdtp * l)); }
-inline double compute_agrav(double om, const Gd& gd) {
+KC_HDI double omega3d(double l, const Gd& gd) { return -(gd.gdtt * l + gd.gdtp) * (1.0 / (gd.gdpp + gd.gdtp * l)); }
+KC_HDI double compute_agrav(double om, const Gd& gd) {
   return kmath::sqrt(kmath::fabs(1.0 / (gd.gdtt + 2.0 * om * gd.gdtp + om * om * gd.gdpp)));
 }
-inline double find_rml(double lam, double a, double lb1, double lb2, double xi) {
+KC_HDI double find_rml(double lam, double a, double lb1, double lb2, double xi) {
   double lamsq = lam * lam;
   auto f = [&](double x) {
     Gd gd = compute_gd(x, kPi2, a);
@@ -99,7 +102,7 @@ inline double find_rml(double lam, double a, double lb1, double lb2, double xi) 
 // tools.c lnf_integrand (puffy.zig:435)
 struct LnfIntegrand {
   double a, lb1, lb2, xi;
-  double operator()(double r) const {
+  KC_HDI double operator()(double r) const {
     double r2 = r * r, r3 = r2 * r, a2 = a * a;
     Gd gd = compute_gd(r, kPi2, a);
     double lam = lam_bl(r, gd, a, lb1, lb2, xi);
@@ -126,23 +129,26 @@ struct LnfIntegrand {
 };
 
 // ---- adaptive Gauss-Kronrod 21 (koral/math/quad.zig; QUADPACK dqk21) --------
-static const double kXgk[11] = {0.995657163025808080735527280689003, 0.973906528517171720077964012084452,
-                                0.930157491355708226001207180059508, 0.865063366688984510732096688423493,
-                                0.780817726586416897063717578345042, 0.679409568299024406234327365114874,
-                                0.562757134668604683339000099272694, 0.433395394129247190799265943165784,
-                                0.294392862701460198131126603103866, 0.148874338981631210884826001129720,
-                                0.000000000000000000000000000000000};
-static const double kWgk[11] = {0.011694638867371874278064396062192, 0.032558162307964727478818972459390,
-                                0.054755896574351996031381300244580, 0.075039674810919952767043140916190,
-                                0.093125454583697605535065465083366, 0.109387158802297641899210590325805,
-                                0.123491976262065851077958109831074, 0.134709217311473325928054001771707,
-                                0.142775938577060080797094273138717, 0.147739104901338491374841515972068,
-                                0.149445554002916905664936468389821};
-static const double kWg[5] = {0.066671344308688137593568809893332, 0.149451349150580593145776339657697,
-                              0.219086362515982043995534934228163, 0.269266719309996355091226921569469,
-                              0.295524224714752870173892994651338};
 template <class F>
-void gk21(const F& f, double a, double b, double& value, double& abserr) {
+KC_HDI void gk21(const F& f, double a, double b, double& value, double& abserr) {
+  const double kXgk[11] = {
+      0.995657163025808080735527280689003, 0.973906528517171720077964012084452,
+      0.930157491355708226001207180059508, 0.865063366688984510732096688423493,
+      0.780817726586416897063717578345042, 0.679409568299024406234327365114874,
+      0.562757134668604683339000099272694, 0.433395394129247190799265943165784,
+      0.294392862701460198131126603103866, 0.148874338981631210884826001129720,
+      0.000000000000000000000000000000000};
+  const double kWgk[11] = {
+      0.011694638867371874278064396062192, 0.032558162307964727478818972459390,
+      0.054755896574351996031381300244580, 0.075039674810919952767043140916190,
+      0.093125454583697605535065465083366, 0.109387158802297641899210590325805,
+      0.123491976262065851077958109831074, 0.134709217311473325928054001771707,
+      0.142775938577060080797094273138717, 0.147739104901338491374841515972068,
+      0.149445554002916905664936468389821};
+  const double kWg[5] = {
+      0.066671344308688137593568809893332, 0.149451349150580593145776339657697,
+      0.219086362515982043995534934228163, 0.269266719309996355091226921569469,
+      0.295524224714752870173892994651338};
   double c = 0.5 * (a + b), h = 0.5 * (b - a);
   double fc = f(c);
   double resg = 0.0, resk = kWgk[10] * fc;
@@ -161,14 +167,16 @@ void gk21(const F& f, double a, double b, double& value, double& abserr) {
   value = resk * h;
   abserr = kmath::fabs((resk - resg) * h);
 }
+// the segment table of the adaptive quadrature: 4 x kMaxSeg doubles of scratch
+constexpr int kMaxSeg = 512;
 template <class F>
-bool integrate(const F& f, double a, double b, double epsabs, double epsrel, double& out) {
+KC_HDI bool integrate(const F& f, double a, double b, double epsabs, double epsrel, double& out, double* seg) {
   if (a == b) {
     out = 0.0;
     return true;
   }
-  const int maxseg = 512;
-  static thread_local double sa[maxseg], sb[maxseg], sv[maxseg], se[maxseg];
+  const int maxseg = kMaxSeg;
+  double *sa = seg, *sb = seg + kMaxSeg, *sv = seg + 2 * kMaxSeg, *se = seg + 3 * kMaxSeg;
   int nseg = 1;
   gk21(f, a, b, sv[0], se[0]);
   sa[0] = a;
@@ -209,7 +217,7 @@ bool integrate(const F& f, double a, double b, double epsabs, double epsrel, dou
 struct TorusConsts {
   double lb1, lb2, lamin, lin, omin, agravin;
 };
-inline TorusConsts torus_consts(double a, const PuffyPhysics& ph) {
+KC_HDI TorusConsts torus_consts(double a, const PuffyPhysics& ph) {
   TorusConsts tc;
   Gd gd = compute_gd(ph.lt_r1, kPi2, a);
   tc.lb1 = lam_bl(ph.lt_r1, gd, a, 0.0, 200000.0, ph.lt_xi);
@@ -225,8 +233,9 @@ inline TorusConsts torus_consts(double a, const PuffyPhysics& ph) {
 struct DsVels {
   double rho, uu, ell;
 };
-// tools.c init_dsandvels_limotorus (puffy.zig:572)
-inline DsVels init_dsandvels(double r, double th, double a, const TorusConsts& tc, const PuffyPhysics& ph) {
+// tools.c init_dsandvels_limotorus (puffy.zig:572); seg: 4 kMaxSeg doubles
+KC_HDI DsVels init_dsandvels_s(double r, double th, double a, const TorusConsts& tc, const PuffyPhysics& ph,
+                               double* seg) {
   DsVels o = {-1.0, 0.0, 0.0};
   double R = r * kmath::sin(th);
   if (R < ph.lt_rin) return o;
@@ -238,7 +247,7 @@ inline DsVels init_dsandvels(double r, double th, double a, const TorusConsts& t
   double rml = find_rml(lam, a, tc.lb1, tc.lb2, ph.lt_xi);
   LnfIntegrand integrand = {a, tc.lb1, tc.lb2, ph.lt_xi};
   double q;
-  bool conv = integrate(integrand, ph.lt_rin, rml, 0.0, 1.0e-12, q);
+  bool conv = integrate(integrand, ph.lt_rin, rml, 0.0, 1.0e-12, q, seg);
   double lnf3d = conv ? q : -kmath::inf();
   double f3d = kmath::exp(-lnf3d);
   const double f3din = 1.0;
@@ -252,8 +261,14 @@ inline DsVels init_dsandvels(double r, double th, double a, const TorusConsts& t
   return o;
 }
 
+// the same with the calling host thread's own scratch
+inline DsVels init_dsandvels(double r, double th, double a, const TorusConsts& tc, const PuffyPhysics& ph) {
+  static thread_local double seg[4 * kMaxSeg];
+  return init_dsandvels_s(r, th, a, tc, ph, seg);
+}
+
 // prepinit.c T from P = bbb T + aaa T^4 (puffy.zig:660)
-inline double t_from_ptot(double P, double aaa, double bbb) {
+KC_HDI double t_from_ptot(double P, double aaa, double bbb) {
   const double third = 0.3333333333333333, twothird = 0.6666666666666666;
   double naw1 = kmath::cbrt(9.0 * aaa * (bbb * bbb) -
                             kmath::sqrt(3.0) * kmath::sqrt(27.0 * (aaa * aaa) * kmath::pow(bbb, 4.0) +
@@ -268,7 +283,7 @@ inline double t_from_ptot(double P, double aaa, double bbb) {
 }
 
 // splitmix64 finalizer (puffy.zig:684)
-inline uint64_t mix64(uint64_t z) {
+KC_HDI uint64_t mix64(uint64_t z) {
   z = z + 0x9E3779B97F4A7C15ULL;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
@@ -276,14 +291,14 @@ inline uint64_t mix64(uint64_t z) {
 }
 // decomposition-invariant cell noise in [-1, 1) (puffy.zig:696 perturbXi);
 // seed 0 is the reference's field, other seeds mix into the x1 word
-inline double perturb_xi(const double x[4], uint64_t seed) {
+KC_HDI double perturb_xi(const double x[4], uint64_t seed) {
   uint64_t b1 = kmath::to_bits(x[1]) ^ seed, b2 = kmath::to_bits(x[2]), b3 = kmath::to_bits(x[3]);
   uint64_t u = mix64(mix64(mix64(b1) ^ b2) ^ b3);
   return 2.0 * ((double)(u >> 11) * 0x1.0p-53) - 1.0;
 }
 
 // atmosphere (relele.c:518/718 atmtype 0, puffy.zig:617-650)
-inline void set_atmospheres(double pp[NV], const Geom& geo, const Geom& gbl, double uintatmmin, double eradatmmin,
+KC_HDI void set_atmospheres(double pp[NV], const Geom& geo, const Geom& gbl, double uintatmmin, double eradatmmin,
                             const PuffyPhysics& ph) {
   double ucon[4];
   normal_obs_velr(geo, ucon);
@@ -305,7 +320,7 @@ inline void set_atmospheres(double pp[NV], const Geom& geo, const Geom& gbl, dou
 
 // prepinit.c per-cell initial primitives (puffy.zig:715 prepInitCellWith)
 // with the optional interior perturbations; A_phi is left in B3.
-inline int prep_init_cell(const Geom& geo, const Geom& gbl, const double jb2m[4][4], const DsVels& dv,
+KC_HDI int prep_init_cell(const Geom& geo, const Geom& gbl, const double jb2m[4][4], const DsVels& dv,
                           const SimParams& sp, const PuffyPhysics& ph, double perturb, double perturb_rho, uint64_t seed,
                           double pp[NV]) {
   const Consts& con = sp.op.c;

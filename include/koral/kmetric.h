@@ -316,7 +316,7 @@ KC_HD double cell_size(const Grid& g, long i, int dim) {
 }
 
 // C calc_Krzysie_at_center with MODYFIKUJKRZYSIE (precompute.zig:30)
-inline void apply_kris_correction(int coords, const MetricParams& mp, const Grid& g, CoordData& d, long ix, long iy,
+KC_HD void apply_kris_correction(int coords, const MetricParams& mp, const Grid& g, CoordData& d, long ix, long iy,
                                   long iz) {
   double xc[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
   double gdet_c = d.gdet;
@@ -375,7 +375,7 @@ KC_HD void geom_from_blocks(const double gblk[20], const double Gblk[20], double
   geom_finish(g);
 }
 // geometry at an arbitrary point (precompute.zig:90 geometryAt)
-inline void geometry_at(int coords, const MetricParams& mp, const double x[4], Geom& geo) {
+KC_HD void geometry_at(int coords, const MetricParams& mp, const double x[4], Geom& geo) {
   CoordData d;
   metric_compute(coords, mp, x, d);
   double gb[20], Gb[20];
@@ -496,7 +496,7 @@ KC_HD void coco_full(const double x[4], int from, int to, const MetricParams& mp
 }
 
 // BL geometry at a cell center (precompute.zig:122 geometryBLat)
-inline void geometry_bl_at(const Grid& gr, const MetricParams& mp, long ix, long iy, long iz, Geom& geo) {
+KC_HD void geometry_bl_at(const Grid& gr, const MetricParams& mp, long ix, long iy, long iz, Geom& geo) {
   double xx[4] = {0.0, grid_xc(gr, ix), grid_yc(gr, iy), grid_zc(gr, iz)};
   double xbl[4];
   mks2_to_bl(xx, mp, xbl);

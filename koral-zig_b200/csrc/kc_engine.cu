@@ -61,6 +61,7 @@ struct kc_handle {
   double t = 0, dt = 0, own_dt = 0, tstepdenmax = 0, tstepdenmin = 1.0e50;
   double min_dx = 0, min_dy = 0, min_dz = 0;
   int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
+  double* init_dv = nullptr;  // the PUFFY init's per-column torus profile
   // block sizes of the per-cell implicit, face-flux and u2p kernels (kc_autotune)
   int tpb_implicit = TPB, tpb_flux = TPB, tpb_u2p = TPB;
   // the step's dt-derived coefficients: pinned host table and its device copy
@@ -148,119 +149,53 @@ T* dalloc(kc_handle* h, size_t n, int& st) {
 // ---- metric cache, host-built once (koral/metric/precompute.zig:175) ----------
 int build_cache(kc_handle* h) {
   const Grid& g = h->gr.g;
-  const MetricParams mp = h->sp.mp;
   long nc = h->gr.nc, sx = h->gr.sx, sy = h->gr.sy, sz = h->gr.sz;
-  std::vector<double> cgc(NGC * nc), cGc(NGCON * nc), kr(NKR * nc), jbl(16 * nc), blg(NBL * nc);
   long ngh = (long)h->gr.ngx * sy * sz;
-  std::vector<double> jb2m(16 * (ngh > 0 ? ngh : 1), 0.0);
-  std::vector<int> asym(sy * sz, 0);
-  long yr = sy, zr = sz;
-  host_par(0, zr * yr, [&](long k) {
-    long iz = k / yr - g.ngz, iy = k % yr - g.ngy;
-    for (long ix = -g.ngx; ix < g.nx + g.ngx; ++ix) {
-      long c = (ix + g.ngx) + (iy + g.ngy) * sx + (iz + g.ngz) * sx * sy;
-      double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
-      CoordData d;
-      metric_compute(MKS2, mp, x, d);
-      apply_kris_correction(MKS2, mp, g, d, ix, iy, iz);
-      for (int i = 0; i < 4; ++i)
-        for (int j = i; j < 4; ++j) {
-          cgc[(long)sym10(i, j) * nc + c] = d.gcov[i][j];
-          if (memcmp(&d.gcov[i][j], &d.gcov[j][i], 8)) asym[k] = 1;
-        }
-      cgc[10L * nc + c] = d.gdet;
-      for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) cGc[(long)(i * 4 + j) * nc + c] = d.gcon[i][j];
-      cGc[16L * nc + c] = d.gttpert;
-      for (int l = 0; l < 4; ++l)
-        for (int m = 0; m < 4; ++m)
-          for (int n = m; n < 4; ++n) {
-            kr[(long)(l * 10 + sym10(m, n)) * nc + c] = d.kris[l][m][n];
-            if (memcmp(&d.kris[l][m][n], &d.kris[l][n][m], 8)) asym[k] = 1;
-          }
-      double m4[4][4];
-      dxdx(x, MKS2, BL, mp, m4);
-      for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) jbl[(long)(i * 4 + j) * nc + c] = m4[i][j];
-      Geom gb;
-      geometry_bl_at(g, mp, ix, iy, iz, gb);
-      for (int i = 0; i < 4; ++i)
-        for (int j = i; j < 4; ++j) {
-          blg[(long)sym10(i, j) * nc + c] = gb.gg[i][j];
-          if (memcmp(&gb.gg[i][j], &gb.gg[j][i], 8)) asym[k] = 1;
-        }
-      for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) blg[(long)(10 + i * 4 + j) * nc + c] = gb.GG[i][j];
-      blg[26L * nc + c] = gb.xx[1];
-      blg[27L * nc + c] = gb.xx[2];
-      if (ix >= g.nx) {
-        long gi = (ix - g.nx) + (long)g.ngx * ((iy + g.ngy) + sy * (iz + g.ngz));
-        double xbl[4] = {0.0, gb.xx[1], gb.xx[2], gb.xx[3]};
-        dxdx(xbl, BL, MKS2, mp, m4);
-        for (int i = 0; i < 4; ++i)
-          for (int j = 0; j < 4; ++j) jb2m[(long)(i * 4 + j) * ngh + gi] = m4[i][j];
-      }
-    }
-  });
-  for (int a : asym)
-    if (a) return fail(h, KC_ERR_INVALID_CONFIG, "metric cache is not bitwise symmetric where the packed layout needs it");
-  std::vector<double> fgc[3], fGc[3];
-  for (int dim = 0; dim < 3; ++dim) {
-    long nf = h->ds.nf[dim];
-    fgc[dim].assign(NGC * nf, 0.0);
-    fGc[dim].assign(NGCON * nf, 0.0);
-  }
-  long yr1 = sy + 1, zr1 = sz + 1;
-  auto put = [&](int dim, long f, const CoordData& d) {
-    long nf = h->ds.nf[dim];
-    for (int i = 0; i < 4; ++i)
-      for (int j = i; j < 4; ++j) fgc[dim][(long)sym10(i, j) * nf + f] = d.gcov[i][j];
-    fgc[dim][10L * nf + f] = d.gdet;
-    for (int i = 0; i < 4; ++i)
-      for (int j = 0; j < 4; ++j) fGc[dim][(long)(i * 4 + j) * nf + f] = d.gcon[i][j];
-    fGc[dim][16L * nf + f] = d.gttpert;
-  };
-  host_par(0, zr1 * yr1, [&](long k) {
-    long iz = k / yr1 - g.ngz, iy = k % yr1 - g.ngy;
-    long nxh = g.nx + g.ngx, nyh = g.ny + g.ngy, nzh = g.nz + g.ngz;
-    for (long ix = -g.ngx; ix <= nxh; ++ix) {
-      long jx = ix + g.ngx, jy = iy + g.ngy, jz = iz + g.ngz;
-      CoordData d;
-      if (iy < nyh && iz < nzh) {
-        double x[4] = {0.0, grid_xl(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
-        metric_compute(MKS2, mp, x, d);
-        put(0, jx + jy * (sx + 1) + jz * sy * (sx + 1), d);
-      }
-      if (ix < nxh && iz < nzh) {
-        double x[4] = {0.0, grid_xc(g, ix), grid_yl(g, iy), grid_zc(g, iz)};
-        metric_compute(MKS2, mp, x, d);
-        put(1, jx + jy * sx + jz * (sy + 1) * sx, d);
-      }
-      if (ix < nxh && iy < nyh) {
-        double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zl(g, iz)};
-        metric_compute(MKS2, mp, x, d);
-        put(2, jx + jy * sx + jz * sy * sx, d);
-      }
-    }
-  });
   int st = 0;
-  auto up = [&](const std::vector<double>& v) -> const double* {
-    double* p = dalloc<double>(h, v.size(), st);
-    if (p) cudaMemcpy(p, v.data(), v.size() * 8, cudaMemcpyHostToDevice);
-    return p;
-  };
-  h->ds.cgc = up(cgc);
-  h->ds.cGc = up(cGc);
-  h->ds.kr = up(kr);
-  h->ds.jbl = up(jbl);
-  h->ds.blg = up(blg);
-  h->ds.jb2m = up(jb2m);
+  CacheOut o;
+  o.cgc = dalloc<double>(h, (size_t)NGC * nc, st);
+  o.cGc = dalloc<double>(h, (size_t)NGCON * nc, st);
+  o.kr = dalloc<double>(h, (size_t)NKR * nc, st);
+  o.jbl = dalloc<double>(h, (size_t)16 * nc, st);
+  o.blg = dalloc<double>(h, (size_t)NBL * nc, st);
+  o.ngh = ngh > 0 ? ngh : 1;
+  o.jb2m = dalloc<double>(h, (size_t)16 * o.ngh, st);
   for (int dim = 0; dim < 3; ++dim) {
-    h->ds.fgc[dim] = up(fgc[dim]);
-    h->ds.fGc[dim] = up(fGc[dim]);
+    o.nf[dim] = h->ds.nf[dim];
+    o.fgc[dim] = dalloc<double>(h, (size_t)NGC * o.nf[dim], st);
+    o.fGc[dim] = dalloc<double>(h, (size_t)NGCON * o.nf[dim], st);
   }
-  return st;
+  o.asym = dalloc<int>(h, 1, st);
+  if (st) return st;
+  k_cache_centers<<<nblk(nc), TPB, 0, h->stream>>>(g, h->sp.mp, sx, sy, sz, o);
+  long nfc = (sx + 1) * (sy + 1) * (sz + 1);
+  for (int dim = 0; dim < 3; ++dim) k_cache_faces<<<nblk(nfc), TPB, 0, h->stream>>>(g, h->sp.mp, sx, sy, sz, dim, o);
+  int asym = 0;
+  st = cuda_check(h, cudaMemcpyAsync(&asym, o.asym, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "metric cache");
+  if (!st) st = cuda_check(h, cudaStreamSynchronize(h->stream), "metric cache");
+  if (st) return st;
+  if (asym) return fail(h, KC_ERR_INVALID_CONFIG, "metric cache is not bitwise symmetric where the packed layout needs it");
+  h->ds.cgc = o.cgc;
+  h->ds.cGc = o.cGc;
+  h->ds.kr = o.kr;
+  h->ds.jbl = o.jbl;
+  h->ds.blg = o.blg;
+  h->ds.jb2m = o.jb2m;
+  for (int dim = 0; dim < 3; ++dim) {
+    h->ds.fgc[dim] = o.fgc[dim];
+    h->ds.fGc[dim] = o.fGc[dim];
+  }
+  return KC_OK;
 }
+
+// a device allocation freed at scope exit (stream-ordered work on it must have
+// completed, which the init's synchronizing read-back ensures)
+struct DevBufE {
+  void* p = nullptr;
+  ~DevBufE() {
+    if (p) cudaFree(p);
+  }
+};
 
 // ---- pass timers -----------------------------------------------------------------
 void pass_mark(kc_handle* h) {
@@ -752,6 +687,58 @@ int run_step(kc_handle* h, double forced_dt, kc_step_info* info) {
     info->nan_cell = -1;
   }
   return st;
+}
+
+// The limotorus profile of (x1, x2) columns [c0, c0 + n) (tools.c
+// init_dsandvels_limotorus, puffy.zig:572: angular-momentum root finding and
+// the adaptive GK21 quadrature of ln f), one thread per column; each thread's
+// quadrature segment table is its slice of `seg` (4 kMaxSeg doubles).
+__global__ void __launch_bounds__(128) k_init_columns(Grid g, MetricParams mp, kcinit::TorusConsts tc,
+                                                      kcinit::PuffyPhysics ph, long c0, long n, double* dvcol,
+                                                      double* seg) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  long col = c0 + k, ix = col % g.nx, iy = col / g.nx;
+  Geom gb0;
+  geometry_bl_at(g, mp, ix, iy, 0, gb0);
+  kcinit::DsVels dv = kcinit::init_dsandvels_s(gb0.xx[1], gb0.xx[2], mp.a, tc, ph, seg + k * 4L * kcinit::kMaxSeg);
+  dvcol[3 * col] = dv.rho;
+  dvcol[3 * col + 1] = dv.uu;
+  dvcol[3 * col + 2] = dv.ell;
+}
+
+// PUFFY per-cell initial state (puffy.zig:715 prepInitCellWith, then the
+// entropy and p2u of initCell, sim.zig:672) on the device, one thread per
+// domain cell, from the host's per-column torus profile dv[3 (ix + nx iy)]
+// (rho, u, ell of init_dsandvels). Ghost cells are left at zero.
+__global__ void __launch_bounds__(128) k_init_cells(DevState s, DevScalars* sc, Grid g, MetricParams mp,
+                                                    const double* dvcol,
+                                                    SimParams sp, kcinit::PuffyPhysics ph, double perturb,
+                                                    double perturb_rho, uint64_t seed) {
+  long nx = g.nx, ny = g.ny, nd = nx * ny * g.nz;
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= nd) return;
+  long ix = d % nx, iy = (d / nx) % ny, iz = d / (nx * ny);
+  double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
+  Geom geo, gbl;
+  geometry_at(MKS2, mp, x, geo);
+  geometry_bl_at(g, mp, ix, iy, iz, gbl);
+  double jac[4][4];
+  double xbl[4] = {0.0, gbl.xx[1], gbl.xx[2], gbl.xx[3]};
+  dxdx(xbl, BL, MKS2, mp, jac);
+  long col = ix + nx * iy;
+  kcinit::DsVels dv = {dvcol[3 * col], dvcol[3 * col + 1], dvcol[3 * col + 2]};
+  double pp[NV], uu[NV];
+  int e = kcinit::prep_init_cell(geo, gbl, jac, dv, sp, ph, perturb, perturb_rho, seed, pp);
+  long c = cidx(s.gr, ix, iy, iz);
+  if (e) {
+    set_err(sc, e, c);
+    return;
+  }
+  pp[ENTR] = s_from_u(pp[RHO], pp[UU], sp.gam);
+  p2u(pp, uu, geo, sp.gam);
+  store_cell(s.p, s.gr.nc, c, pp);
+  store_cell(s.u, s.gr.nc, c, uu);
 }
 
 }  // namespace
@@ -1288,42 +1275,35 @@ int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t see
   kcinit::PuffyPhysics ph;
   ph.mass = h->opt.mass;
   kcinit::TorusConsts tc = kcinit::torus_consts(mp.a, ph);
-  std::vector<double> hp((size_t)NV * nc, 0.0), hu((size_t)NV * nc, 0.0);
-  std::vector<int> errs((size_t)g.nx * g.ny, 0);
-  const double gam = h->sp.gam;
-  host_par(0, (long)g.nx * g.ny, [&](long k) {
-    long ix = k % g.nx, iy = k / g.nx;
-    Geom gb0;
-    geometry_bl_at(g, mp, ix, iy, 0, gb0);
-    kcinit::DsVels dv = kcinit::init_dsandvels(gb0.xx[1], gb0.xx[2], mp.a, tc, ph);
-    for (long iz = 0; iz < g.nz; ++iz) {
-      double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
-      Geom geo, gbl;
-      geometry_at(MKS2, mp, x, geo);
-      geometry_bl_at(g, mp, ix, iy, iz, gbl);
-      double jac[4][4];
-      double xbl[4] = {0.0, gbl.xx[1], gbl.xx[2], gbl.xx[3]};
-      dxdx(xbl, BL, MKS2, mp, jac);
-      long c = (ix + g.ngx) + (iy + g.ngy) * gr.sx + (iz + g.ngz) * gr.sx * gr.sy;
-      double* pp = &hp[(size_t)c * NV];
-      int e = kcinit::prep_init_cell(geo, gbl, jac, dv, h->sp, ph, perturb, perturb_rho, seed, pp);
-      if (e) {
-        errs[k] = e;
-        return;
-      }
-      pp[ENTR] = s_from_u(pp[RHO], pp[UU], gam);
-      p2u(pp, &hu[(size_t)c * NV], geo, gam);
-    }
-  });
-  for (int e : errs)
-    if (e) return fail(h, e, "PUFFY init: a torus cell failed its velocity conversion");
   h->last_status = 0;
   h->err.clear();
-  int st = cuda_check(h, cudaMemsetAsync(h->ds.flags, 0, 6L * nc * sizeof(int), h->stream), "init");
-  if (!st) st = cuda_check(h, cudaMemsetAsync(h->ds.vecpot, 0, 6L * nc * sizeof(double), h->stream), "init");
-  if (!st) st = upload_field(h, h->ds.p, hp.data(), NV);
-  if (!st) st = upload_field(h, h->ds.u, hu.data(), NV);
+  // the torus profile per (x1, x2) column (the metric is axisymmetric, so one
+  // solve serves a column), in chunks whose quadrature scratch stays <= 1 GiB
+  long ncol = (long)g.nx * g.ny;
+  int st = 0;
+  if (!h->init_dv) h->init_dv = dalloc<double>(h, (size_t)3 * ncol, st);
   if (st) return st;
+  double* ddv = h->init_dv;
+  const long chunk = 65536;
+  long nseg = ncol < chunk ? ncol : chunk;
+  DevBufE seg;
+  if (cudaMalloc(&seg.p, (size_t)nseg * 4 * kcinit::kMaxSeg * 8) != cudaSuccess)
+    return fail(h, KC_ERR_OOM, "init quadrature scratch");
+  for (long c0 = 0; c0 < ncol; c0 += chunk) {
+    long n = ncol - c0 < chunk ? ncol - c0 : chunk;
+    k_init_columns<<<nblk(n), TPB, 0, h->stream>>>(g, mp, tc, ph, c0, n, ddv, (double*)seg.p);
+  }
+  st = cuda_check(h, cudaMemsetAsync(h->ds.flags, 0, 6L * nc * sizeof(int), h->stream), "init");
+  if (!st) st = cuda_check(h, cudaMemsetAsync(h->ds.vecpot, 0, 6L * nc * sizeof(double), h->stream), "init");
+  if (!st) st = cuda_check(h, cudaMemsetAsync(h->ds.p, 0, (size_t)NV * nc * 8, h->stream), "init");
+  if (!st) st = cuda_check(h, cudaMemsetAsync(h->ds.u, 0, (size_t)NV * nc * 8, h->stream), "init");
+  if (st) return st;
+  const double gam = h->sp.gam;
+  reset_step_scalars(h);
+  k_init_cells<<<nblk((long)g.nx * g.ny * g.nz), TPB, 0, h->stream>>>(h->ds, h->dsc, g, mp, ddv, h->sp, ph, perturb,
+                                                                       perturb_rho, seed);
+  // a failed torus cell is reported through the device scalars' error slot
+  if ((st = sync_check(h, "init")) || (st = collect_step_scalars(h, false))) return st;
   reset_step_scalars(h);
   launch_set_bc(h);
   long my = gr.ny == 1 ? 1 : gr.ny + 1, mz = gr.nz == 1 ? 1 : gr.nz + 1;

@@ -48,6 +48,102 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
   int v = (int)(t % nv);
   aos[t] = soa[(long)v * nc + c];
 }
+// ---- the metric cache, built on the device (koral/metric/precompute.zig:175) ----
+// The same per-point code as the host build of the oracle (dual-number metric,
+// MODYFIKUJKRZYSIE correction, BL geometry and Jacobians), one thread per cell
+// (ghosts included) or per face. Symmetry of the packed layouts is checked
+// bitwise and reported through *asym.
+struct CacheOut {
+  double *cgc, *cGc, *kr, *jbl, *blg, *jb2m;
+  double *fgc[3], *fGc[3];
+  long nf[3], ngh;
+  int* asym;
+};
+__global__ void __launch_bounds__(128) k_cache_centers(Grid g, MetricParams mp, long sx, long sy, long sz, CacheOut o) {
+  long nc = sx * sy * sz;
+  long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  long ix = c % sx - g.ngx, iy = (c / sx) % sy - g.ngy, iz = c / (sx * sy) - g.ngz;
+  double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
+  CoordData d;
+  metric_compute(MKS2, mp, x, d);
+  apply_kris_correction(MKS2, mp, g, d, ix, iy, iz);
+  int asym = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) {
+      o.cgc[(long)sym10(i, j) * nc + c] = d.gcov[i][j];
+      if (dbits(d.gcov[i][j]) != dbits(d.gcov[j][i])) asym = 1;
+    }
+  o.cgc[10L * nc + c] = d.gdet;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) o.cGc[(long)(i * 4 + j) * nc + c] = d.gcon[i][j];
+  o.cGc[16L * nc + c] = d.gttpert;
+  for (int l = 0; l < 4; ++l)
+    for (int m = 0; m < 4; ++m)
+      for (int n = m; n < 4; ++n) {
+        o.kr[(long)(l * 10 + sym10(m, n)) * nc + c] = d.kris[l][m][n];
+        if (dbits(d.kris[l][m][n]) != dbits(d.kris[l][n][m])) asym = 1;
+      }
+  double m4[4][4];
+  dxdx(x, MKS2, BL, mp, m4);
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) o.jbl[(long)(i * 4 + j) * nc + c] = m4[i][j];
+  Geom gb;
+  geometry_bl_at(g, mp, ix, iy, iz, gb);
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) {
+      o.blg[(long)sym10(i, j) * nc + c] = gb.gg[i][j];
+      if (dbits(gb.gg[i][j]) != dbits(gb.gg[j][i])) asym = 1;
+    }
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) o.blg[(long)(10 + i * 4 + j) * nc + c] = gb.GG[i][j];
+  o.blg[26L * nc + c] = gb.xx[1];
+  o.blg[27L * nc + c] = gb.xx[2];
+  if (ix >= g.nx) {
+    long gi = (ix - g.nx) + (long)g.ngx * ((iy + g.ngy) + sy * (iz + g.ngz));
+    double xbl[4] = {0.0, gb.xx[1], gb.xx[2], gb.xx[3]};
+    dxdx(xbl, BL, MKS2, mp, m4);
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) o.jb2m[(long)(i * 4 + j) * o.ngh + gi] = m4[i][j];
+  }
+  if (asym) atomicOr(o.asym, 1);
+}
+__device__ __forceinline__ void cache_put_face(const CacheOut& o, int dim, long f, const CoordData& d) {
+  long nf = o.nf[dim];
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) o.fgc[dim][(long)sym10(i, j) * nf + f] = d.gcov[i][j];
+  o.fgc[dim][10L * nf + f] = d.gdet;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) o.fGc[dim][(long)(i * 4 + j) * nf + f] = d.gcon[i][j];
+  o.fGc[dim][16L * nf + f] = d.gttpert;
+}
+// faces of direction `dim` at lower corners (ix, iy, iz) over (sx+1)(sy+1)(sz+1)
+__global__ void __launch_bounds__(128) k_cache_faces(Grid g, MetricParams mp, long sx, long sy, long sz, int dim,
+                                                     CacheOut o) {
+  long n = (sx + 1) * (sy + 1) * (sz + 1);
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  long jx = t % (sx + 1), jy = (t / (sx + 1)) % (sy + 1), jz = t / ((sx + 1) * (sy + 1));
+  long ix = jx - g.ngx, iy = jy - g.ngy, iz = jz - g.ngz;
+  long nxh = g.nx + g.ngx, nyh = g.ny + g.ngy, nzh = g.nz + g.ngz;
+  CoordData d;
+  if (dim == 0 && iy < nyh && iz < nzh) {
+    double x[4] = {0.0, grid_xl(g, ix), grid_yc(g, iy), grid_zc(g, iz)};
+    metric_compute(MKS2, mp, x, d);
+    cache_put_face(o, 0, jx + jy * (sx + 1) + jz * sy * (sx + 1), d);
+  }
+  if (dim == 1 && ix < nxh && iz < nzh) {
+    double x[4] = {0.0, grid_xc(g, ix), grid_yl(g, iy), grid_zc(g, iz)};
+    metric_compute(MKS2, mp, x, d);
+    cache_put_face(o, 1, jx + jy * sx + jz * (sy + 1) * sx, d);
+  }
+  if (dim == 2 && ix < nxh && iy < nyh) {
+    double x[4] = {0.0, grid_xc(g, ix), grid_yc(g, iy), grid_zl(g, iz)};
+    metric_compute(MKS2, mp, x, d);
+    cache_put_face(o, 2, jx + jy * sx + jz * sy * sx, d);
+  }
+}
+
 // KDMP body (dump.zig:122 serializePrimBody): the domain primitives in
 // [iz][iy][ix][iv] order, one thread per output double (coalesced writes)
 __global__ void k_domain_to_kdmp(DevState s, double* __restrict__ body) {

@@ -64,7 +64,7 @@ KC_HDM void invert4(const double a_in[4][4], double inv[4][4]) {
       perm[piv] = tp;
     }
     for (int r = k + 1; r < 4; ++r) {
-      lu[r][k] /= lu[k][k];
+      lu[r][k] = kmath::div(lu[r][k], lu[k][k]);
       for (int cc = k + 1; cc < 4; ++cc) lu[r][cc] -= lu[r][k] * lu[k][cc];
     }
   }
@@ -77,7 +77,7 @@ KC_HDM void invert4(const double a_in[4][4], double inv[4][4]) {
     for (int r = 3; r >= 0; --r) {
       x[r] = y[r];
       for (int cc = r + 1; cc < 4; ++cc) x[r] -= lu[r][cc] * x[cc];
-      x[r] /= lu[r][r];
+      x[r] = kmath::div(x[r], lu[r][r]);
     }
     for (int rr = 0; rr < 4; ++rr) inv[rr][col] = x[rr];
   }
@@ -332,6 +332,7 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
       success = true;
       break;
     }
+    KC_ROLLED
     for (int j = 0; j < 4; ++j) {
       double sign = -1.0;
       while (true) {
@@ -484,6 +485,7 @@ KC_HDN ImplicitResult implicit_ladder(double uu[NV], double pp[NV], const Geom& 
     double od = 1.0;
     for (int i = 0; i < level; ++i) od /= ip.opdamp_factor;
     opl.opdamp = od;
+    KC_ROLLED
     for (int ir = 0; ir < 6; ++ir) {
       int p, e, fr;
       implicit_rung(ir, pre.startwith, p, e, fr);

@@ -409,20 +409,18 @@ KC_HDM double m1_gammarel2(const Geom& g, const double av[4]) {
   double den = gn11 * (rdtt * rdtt) + 2.0 * gn12 * rdtt * rdtx + gn22 * (rdtx * rdtx) + 2.0 * gn13 * rdtt * rdty +
                2.0 * gn23 * rdtx * rdty + gn33 * (rdty * rdty) + 2.0 * (gn14 * rdtt + gn24 * rdtx + gn34 * rdty) * rdtz +
                gn44 * (rdtz * rdtz);
-  double gamma2a = (-0.25 * (2.0 * (gn11 * gn11) * (rdtt * rdtt) + mix * (mix + sq) +
+  double gamma2a = kmath::div((-0.25 * (2.0 * (gn11 * gn11) * (rdtt * rdtt) + mix * (mix + sq) +
                              gn11 * (4.0 * gn12 * rdtt * rdtx + gn22 * (rdtx * rdtx) + 2.0 * gn23 * rdtx * rdty +
                                      gn33 * (rdty * rdty) + 2.0 * gn24 * rdtx * rdtz + 2.0 * gn34 * rdty * rdtz +
-                                     gn44 * (rdtz * rdtz) + rdtt * (4.0 * gn13 * rdty + 4.0 * gn14 * rdtz + sq)))) /
-                   den;
+                                     gn44 * (rdtz * rdtz) + rdtt * (4.0 * gn13 * rdty + 4.0 * gn14 * rdtz + sq)))), den);
   double gamma2;
   if (gamma2a < gsl || !kmath::isfinite(gamma2a)) {
-    double gamma2b = (0.25 * (-2.0 * (gn11 * gn11) * (rdtt * rdtt) -
+    double gamma2b = kmath::div((0.25 * (-2.0 * (gn11 * gn11) * (rdtt * rdtt) -
                               1.0 * gn11 *
                                   (4.0 * gn12 * rdtt * rdtx + gn22 * (rdtx * rdtx) +
                                    rdty * (4.0 * gn13 * rdtt + 2.0 * gn23 * rdtx + gn33 * rdty) +
                                    2.0 * (2.0 * gn14 * rdtt + gn24 * rdtx + gn34 * rdty) * rdtz + gn44 * (rdtz * rdtz)) +
-                              gn11 * rdtt * sq + mix * (-1.0 * gn12 * rdtx - 1.0 * gn13 * rdty - 1.0 * gn14 * rdtz + sq))) /
-                     den;
+                              gn11 * rdtt * sq + mix * (-1.0 * gn12 * rdtx - 1.0 * gn13 * rdty - 1.0 * gn14 * rdtz + sq))), den);
     gamma2 = gamma2b;
   } else {
     gamma2 = gamma2a;
@@ -439,7 +437,7 @@ KC_HDM void m1_cold(const Geom& g, const double av_in[4], double gammarel2, doub
   double gn33 = g.GG[2][2], gn34 = g.GG[2][3], gn44 = g.GG[3][3];
   double alpha = g.alpha;
   double rdtx = av_in[1], rdty = av_in[2], rdtz = av_in[3];
-  double utsq = gammarel2 / (alpha * alpha);
+  double utsq = kmath::div(gammarel2, (alpha * alpha));
   for (int i = 0; i < 4; ++i) av[i] = av_in[i];
   double mix = gn13 * rdty + gn14 * rdtz;
   double disc = kmath::sqrt(((gn12 * gn12) * (rdtx * rdtx) + 2.0 * gn12 * rdtx * mix + mix * mix -
@@ -447,17 +445,15 @@ KC_HDM void m1_cold(const Geom& g, const double av_in[4], double gammarel2, doub
                                  (gn22 * (rdtx * rdtx) + 2.0 * gn23 * rdtx * rdty + gn33 * (rdty * rdty) +
                                   2.0 * gn24 * rdtx * rdtz + 2.0 * gn34 * rdty * rdtz + gn44 * (rdtz * rdtz))) *
                             utsq * (gn11 + utsq) * ((gn11 + 4.0 * utsq) * (gn11 + 4.0 * utsq)));
-  av[0] = (0.25 * (-4.0 * (gn12 * rdtx + gn13 * rdty + gn14 * rdtz) * utsq * (gn11 + utsq) + disc)) /
-          (gn11 * utsq * (gn11 + utsq));
-  erf = (0.75 * disc) / (utsq * (gn11 + utsq) * (gn11 + 4.0 * utsq));
+  av[0] = kmath::div((0.25 * (-4.0 * (gn12 * rdtx + gn13 * rdty + gn14 * rdtz) * utsq * (gn11 + utsq) + disc)), (gn11 * utsq * (gn11 + utsq)));
+  erf = kmath::div((0.75 * disc), (utsq * (gn11 + utsq) * (gn11 + 4.0 * utsq)));
   double avcon[4];
   raise_vec(av, g, avcon);
   double gammarel = kmath::sqrt(gammarel2);
   for (int i = 0; i < 4; ++i) urfconrel[i] = 0.0;
   if (erf > 0.0) {
     for (int jj = 1; jj < 4; ++jj)
-      urfconrel[jj] = alpha * (avcon[jj] + 1.0 / 3.0 * erf * g.GG[0][jj] * (4.0 * gammarel2 - 1.0)) /
-                      (4.0 / 3.0 * erf * gammarel);
+      urfconrel[jj] = kmath::div(alpha * (avcon[jj] + 1.0 / 3.0 * erf * g.GG[0][jj] * (4.0 * gammarel2 - 1.0)), (4.0 / 3.0 * erf * gammarel));
   }
 }
 
@@ -471,21 +467,20 @@ KC_HDN U2pRadRes u2p_rad(const double uu[NV], double pp[NV], const Geom& g, cons
   const double numepsilon = 2.220446049250313e-16;
   double gdetu = g.gdet;
   double alpha = g.alpha;
-  double avcov[4] = {uu[EE] / gdetu, uu[FX] / gdetu, uu[FY] / gdetu, uu[FZ] / gdetu};
+  double avcov[4] = {kmath::div(uu[EE], gdetu), kmath::div(uu[FX], gdetu), kmath::div(uu[FY], gdetu), kmath::div(uu[FZ], gdetu)};
   double avcon[4];
   raise_vec(avcov, g, avcon);
   double gammarel2 = m1_gammarel2(g, avcov);
-  double erf = 3.0 * avcon[0] * alpha * alpha / (4.0 * gammarel2 - 1.0);
+  double erf = kmath::div(3.0 * avcon[0] * alpha * alpha, (4.0 * gammarel2 - 1.0));
   double gammamax = rp.gammamaxrad;
-  bool nonfailure = gammarel2 >= 1.0 && erf > rp.eradfloor && gammarel2 <= gammamax * gammamax / gsl / gsl;
+  bool nonfailure = gammarel2 >= 1.0 && erf > rp.eradfloor && gammarel2 <= kmath::div(kmath::div(gammamax * gammamax, gsl), gsl);
   double urfcon[4];
   bool corrected = false;
   U2pRadRes res;
   if (nonfailure) {
     double gammarel = kmath::sqrt(gammarel2);
     for (int ii = 0; ii < 4; ++ii)
-      urfcon[ii] = alpha * (avcon[ii] + 1.0 / 3.0 * erf * g.GG[0][ii] * (4.0 * gammarel2 - 1.0)) /
-                   (4.0 / 3.0 * erf * gammarel);
+      urfcon[ii] = kmath::div(alpha * (avcon[ii] + 1.0 / 3.0 * erf * g.GG[0][ii] * (4.0 * gammarel2 - 1.0)), (4.0 / 3.0 * erf * gammarel));
   } else {
     double one_eps = 1.0 + 10.0 * numepsilon;
     double s_av[4], s_erf, s_urf[4], f_av[4], f_erf, f_urf[4];
@@ -523,7 +518,7 @@ KC_HDN U2pRadRes u2p_rad(const double uu[NV], double pp[NV], const Geom& g, cons
 KC_HDM int check_floors_rad(double pp[NV], const Geom& g, const RadParams& rp) {
   int ret = 0;
   double ehat = -calc_ff_rtt(pp, g, nullptr);
-  double eratio = pp[EE] / ehat;
+  double eratio = kmath::div(pp[EE], ehat);
   if (pp[EE] < rp.eradfloor) {
     pp[EE] = rp.eradfloor;
     ret = -1;
@@ -533,7 +528,7 @@ KC_HDM int check_floors_rad(double pp[NV], const Geom& g, const RadParams& rp) {
     ret = -1;
   }
   if (ehat > rp.eerhoratiomax * pp[RHO]) {
-    pp[RHO] = 1.0 / rp.eerhoratiomax * ehat;
+    pp[RHO] = kmath::div(1.0, rp.eerhoratiomax) * ehat;
     ret = -1;
   }
   if (ehat < rp.eeuuratiomin * pp[UU]) {
@@ -541,7 +536,7 @@ KC_HDM int check_floors_rad(double pp[NV], const Geom& g, const RadParams& rp) {
     ret = -1;
   }
   if (ehat > rp.eeuuratiomax * pp[UU]) {
-    pp[UU] = 1.0 / rp.eeuuratiomax * ehat;
+    pp[UU] = kmath::div(1.0, rp.eeuuratiomax) * ehat;
     ret = -1;
   }
   return ret;

@@ -33,12 +33,15 @@
 #define KC_HD __host__ __device__ __forceinline__
 #define KC_HDN __host__ __device__ __noinline__
 #define KC_HDI __host__ __device__ inline  // host and device, inlining left to the compiler
+// a loop kept rolled on the device (code size: the solver is instruction-fetch bound)
+#define KC_ROLLED _Pragma("unroll 1")
 #else
 #include <string.h>
 #include <math.h>
 #define KC_HD inline
 #define KC_HDN inline
 #define KC_HDI inline
+#define KC_ROLLED
 #endif
 // Mid-size helpers (p2u, the M1 closure, boosts, opacities' thermodynamics,
 // the 4x4 inverse): inlined unless KC_SHARED_HELPERS is 1, which compiles

@@ -281,7 +281,7 @@ KC_HD void lorentz_from_pair(const double ucon[4], const double ucov[4], const d
     }
 }
 KC_HD void normal_obs_concov(const Geom& g, double con[4], double cov[4]) {
-  double alpha = kmath::sqrt(-1.0 / g.GG[0][0]);
+  double alpha = kmath::sqrt(kmath::div(-1.0, g.GG[0][0]));
   cov[0] = -alpha;
   cov[1] = 0.0;
   cov[2] = 0.0;

@@ -39,7 +39,7 @@ KC_HD double my_sign(double x) {
 }
 
 // 4x4 LU inversion with partial pivoting, no error path (implicit.zig:172)
-KC_HDM void invert4(const double a_in[4][4], double inv[4][4]) {
+KC_HDN void invert4(const double a_in[4][4], double inv[4][4]) {
   double lu[4][4];
   int perm[4] = {0, 1, 2, 3};
   for (int i = 0; i < 4; ++i)

@@ -3,6 +3,8 @@ CPU oracle: the per-cell batch entry points on the reference's golden record
 inputs, and whole RK2IMEX steps from the reference's post-init self-golden
 states. The plain FP64 engine is built without FMA contraction and shares the
 oracle's per-point source, so every comparison here is bit for bit."""
+import os
+
 import numpy as np
 import pytest
 
@@ -254,3 +256,24 @@ def test_autotune_restores_state_and_keeps_bits():
         b.step()
     assert np.array_equal(a.p, b.p) and np.array_equal(a.u, b.u) and np.array_equal(a.flags, b.flags)
     assert a.counters() == b.counters()
+
+
+def test_production_2d_grid_ten_steps_bitwise():
+    """The 2D production configuration (384x360 PUFFY grid, the engine's own
+    init, 10 CFL steps in the graph form): every state and counter identical to
+    the oracle's after each step."""
+    kc = _kc()
+    grid = kc.puffy_grid(384, 360)
+    gpu = kc.Sim(grid, kc.puffy_options())
+    orc = OracleSim(grid, kc.puffy_options(), nthreads=os.cpu_count() or 1)
+    assert gpu.initPuffy() == orc.init_puffy()
+    orc.lib.orc_sim_init_timestep_guess(orc.h)
+    _assert_same_state(gpu, orc)
+    gpu.set_graph(True)
+    for _ in range(10):
+        gpu.step()
+        orc.step()
+        _assert_same_state(gpu, orc)
+    cg, co = gpu.counters(), orc.counters()
+    for k in ["t", "dt", "tstepdenmax", "tstepdenmin", "n_radimp_failures", "n_radimp_iters", "n_radimp_solves"]:
+        assert cg[k] == co[k], (k, cg[k], co[k])

@@ -400,7 +400,9 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
       } else {
         xiapp /= ip.damping_factor;
       }
-      if (xiapp < ip.max_damping) {
+      // !(x >= m) is x < m for every number and also true for NaN: a NaN
+      // damping factor (a NaN start state) fails the rung instead of looping
+      if (!(xiapp >= ip.max_damping)) {
         failed = true;
         break;
       }

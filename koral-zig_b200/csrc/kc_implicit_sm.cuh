@@ -400,7 +400,7 @@ __device__ __noinline__ int imp_advance(ImpLane& L, const ImpParams& P) {
         } else {
           L.xiapp /= ip.damping_factor;
         }
-        if (L.xiapp < ip.max_damping) {
+        if (!(L.xiapp >= ip.max_damping)) {  // NaN fails the rung (see solve_4dprim_core)
           L.failed = true;
           L.st = S_C_CONV;
         } else {

@@ -239,13 +239,16 @@ int kc_set_implicit_mode(kc_handle* h, int32_t mode);
 int kc_set_graph(kc_handle* h, int32_t on);
 
 /* The autotuner's choice (no reference counterpart): implicit form
- * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT) and threads per block of the
- * per-cell implicit, face-flux and u2p kernels, with the measured step time of
- * the choice and of the configuration on entry. */
+ * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT), threads per block of the
+ * per-cell implicit, face-flux and u2p kernels, and on 3D grids the per-cell
+ * implicit kernel's thread -> cell order (1: phi fastest, the default, so that
+ * a warp's cells share r and theta; 0: x fastest), with the measured step time
+ * of the choice and of the configuration on entry. */
 typedef struct kc_tune_result {
   int32_t implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
   double ms_per_step, ms_per_step_entry;
   int32_t trials;
+  int32_t implicit_phi_fastest;
 } kc_tune_result;
 /* Times whole steps on the handle's current state for each candidate, one
  * knob at a time, and keeps the fastest configuration set; the state and the

@@ -64,6 +64,15 @@ struct kc_handle {
   double* init_dv = nullptr;  // the PUFFY init's per-column torus profile
   // block sizes of the per-cell implicit, face-flux and u2p kernels (kc_autotune)
   int tpb_implicit = TPB, tpb_flux = TPB, tpb_u2p = TPB;
+#ifndef KC_IMPLICIT_PHI_FASTEST
+#define KC_IMPLICIT_PHI_FASTEST 1
+#endif
+#ifndef KC_U2P_PHI_FASTEST
+#define KC_U2P_PHI_FASTEST 0
+#endif
+  // thread -> cell order of the per-cell implicit and u2p kernels on 3D grids:
+  // phi fastest (warps of cells sharing r and theta) or x fastest
+  int implicit_phi_fastest = KC_IMPLICIT_PHI_FASTEST, u2p_phi_fastest = KC_U2P_PHI_FASTEST;
   // the step's dt-derived coefficients: pinned host table and its device copy
   // (DevState::coef); slots 0-3 are fixed by run_step, later ones appended
   double* coef_host = nullptr;
@@ -293,7 +302,8 @@ void launch_calc_u2p(kc_handle* h) {
   PassScope ps(h, KC_PASS_U2P);
   cudaMemsetAsync(&h->dsc->any_hd, 0, sizeof(int), h->stream);
   ++h->n_launch;
-  k_u2p<<<nblk(ndom, h->tpb_u2p), h->tpb_u2p, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, h->sp.fl, h->sp.rp, pnc);
+  k_u2p<<<nblk(ndom, h->tpb_u2p), h->tpb_u2p, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam, h->sp.fl, h->sp.rp, pnc,
+                                                                h->u2p_phi_fastest && gr.nz > 1);
   if (h->sp.do_fixups) {
     PassScope pf(h, KC_PASS_FIXUP);
     ++h->n_launch;
@@ -322,6 +332,7 @@ void launch_implicit(kc_handle* h, int dt_slot) {
   a.op = h->sp.op;
   a.ip = h->sp.ip;
   a.polar_nc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
+  a.phi_fastest = h->implicit_phi_fastest && gr.nz > 1;
   PassScope ps(h, KC_PASS_IMPLICIT);
   // the learned guess and the harvest run in the per-cell form
   bool extra = h->guess_mode == KC_GUESS_MLP || h->hcap > 0;
@@ -1902,17 +1913,18 @@ extern "C" int kc_fp64_peak(double* tflops) {
 // ---- autotuner -------------------------------------------------------------------
 namespace {
 struct TuneConfig {
-  int implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
+  int implicit_mode, tpb_implicit, tpb_flux, tpb_u2p, phi_fastest;
 };
 void tune_apply(kc_handle* h, const TuneConfig& c) {
   h->opt.implicit_mode = c.implicit_mode;
+  h->implicit_phi_fastest = c.phi_fastest;
   h->tpb_implicit = c.tpb_implicit;
   h->tpb_flux = c.tpb_flux;
   h->tpb_u2p = c.tpb_u2p;
   drop_graph(h);
 }
 TuneConfig tune_current(const kc_handle* h) {
-  return {h->opt.implicit_mode, h->tpb_implicit, h->tpb_flux, h->tpb_u2p};
+  return {h->opt.implicit_mode, h->tpb_implicit, h->tpb_flux, h->tpb_u2p, h->implicit_phi_fastest};
 }
 // The state a step reads and writes across steps: p, u, flags on the device and
 // the handle's step scalars and counters.
@@ -1940,8 +1952,9 @@ void tune_restore(kc_handle* h, const TuneSnapshot& sn) {
 }
 }  // namespace
 
-// Picks the implicit form (per-cell or split) and the block sizes of the
-// per-cell implicit, face-flux and u2p kernels by timing whole steps on the
+// Picks the implicit form (per-cell or split), the block sizes of the
+// per-cell implicit, face-flux and u2p kernels and (3D) the per-cell implicit
+// kernel's cell order (phi or x fastest) by timing whole steps on the
 // handle's current state, one knob at a time (coordinate descent from the
 // configuration on entry). Each trial restores the state, runs one untimed step
 // (with the graph form on, a second one, so the timed steps replay the graph)
@@ -1994,14 +2007,16 @@ extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
   entry_ms = best_ms;
   const int forms[2] = {KC_IMPLICIT_PER_CELL, KC_IMPLICIT_SPLIT};
   const int sizes[3] = {64, 96, 128};
-  for (int knob = 0; knob < 4 && !st; ++knob) {
-    int n = knob == 0 ? 2 : 3;
+  for (int knob = 0; knob < 5 && !st; ++knob) {
+    if (knob == 4 && h->gr.nz == 1) break;  // the cell order matters on 3D grids only
+    int n = (knob == 0 || knob == 4) ? 2 : 3;
     for (int i = 0; i < n && !st; ++i) {
       TuneConfig c = best;
       if (knob == 0) c.implicit_mode = forms[i];
       if (knob == 1) c.tpb_implicit = sizes[i];
       if (knob == 2) c.tpb_flux = sizes[i];
       if (knob == 3) c.tpb_u2p = sizes[i];
+      if (knob == 4) c.phi_fastest = i;
       if (memcmp(&c, &best, sizeof c) == 0) continue;
       double ms = 0.0;
       st = measure(c, ms);
@@ -2025,6 +2040,7 @@ extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
     out->tpb_implicit = best.tpb_implicit;
     out->tpb_flux = best.tpb_flux;
     out->tpb_u2p = best.tpb_u2p;
+    out->implicit_phi_fastest = best.phi_fastest;
     out->ms_per_step = best_ms;
     out->ms_per_step_entry = entry_ms;
     out->trials = trials;

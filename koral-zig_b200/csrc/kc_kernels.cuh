@@ -22,6 +22,18 @@ __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned
 struct Range {
   long x0, y0, z0, nx, ny, nz;
 };
+// The domain cell of this thread with phi (z) fastest: the cells of a warp then
+// share (r, theta), and on an axisymmetric torus they take nearly the same path
+// through a per-cell solver (the implicit solve, the u2p inversion).
+__device__ __forceinline__ bool domain_cell_phi_fastest(const DGrid& gr, long& ix, long& iy, long& iz) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)gr.nx * gr.ny * gr.nz) return false;
+  iz = t % gr.nz;
+  long q = t / gr.nz;
+  ix = q % gr.nx;
+  iy = q / gr.nx;
+  return true;
+}
 __device__ __forceinline__ bool range_cell(const Range& r, long& ix, long& iy, long& iz) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long n = r.nx * r.ny * r.nz;
@@ -235,10 +247,14 @@ __global__ void __launch_bounds__(128) k_update_entropy(DevState s, double gam) 
 
 // ---- u2p (koral/sim.zig:924-1000) --------------------------------------------
 __global__ void __launch_bounds__(128) k_u2p(DevState s, DevScalars* sc, double gam, FloorParams fl, RadParams rp,
-                                             int polar_nc) {
+                                             int polar_nc, int phi_fastest) {
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
-  if (!range_cell(r, ix, iy, iz)) return;
+  if (phi_fastest) {
+    if (!domain_cell_phi_fastest(s.gr, ix, iy, iz)) return;
+  } else if (!range_cell(r, ix, iy, iz)) {
+    return;
+  }
   long c = cidx(s.gr, ix, iy, iz), nc = s.gr.nc;
   double uu[NV], pp[NV];
   load_cell(s.u, nc, c, uu);
@@ -965,6 +981,7 @@ __global__ void __launch_bounds__(128) k_update(DevState s, double gam, int dt_s
 struct ImplArgs {
   double gam;
   int dt_slot;  // the pass's dt in DevState::coef
+  int phi_fastest;  // thread -> cell order of the per-cell kernel: 1 = phi fastest, 0 = x fastest
   RadParams rp;
   OpacParams op;
   ImplicitParams ip;
@@ -991,9 +1008,13 @@ template <bool EXTRA>
 __global__ void __launch_bounds__(128, KC_IMPLICIT_MIN_BLOCKS) k_implicit(DevState s, DevScalars* sc, ImplArgs a,
                                                                           ImplExtra x) {
   const double dt = s.coef[a.dt_slot];
-  Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
-  if (!range_cell(r, ix, iy, iz)) return;
+  if (a.phi_fastest) {
+    if (!domain_cell_phi_fastest(s.gr, ix, iy, iz)) return;
+  } else {
+    Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
+    if (!range_cell(r, ix, iy, iz)) return;
+  }
   if (a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) return;
   long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
   double uu[NV], pp[NV];

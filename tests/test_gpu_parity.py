@@ -249,6 +249,7 @@ def test_autotune_restores_state_and_keeps_bits():
     assert r["implicit_mode"] in (0, 2) and r["trials"] >= 2
     for k in ("tpb_implicit", "tpb_flux", "tpb_u2p"):
         assert r[k] in (64, 96, 128)
+    assert r["implicit_phi_fastest"] in (0, 1)
     assert np.array_equal(b.p, p0) and b.counters() == c0
     b.set_graph(True)
     for _ in range(3):

@@ -9,6 +9,23 @@
 #include "kc_mixed.cuh"
 #include "kc_mlp.cuh"
 
+// Resident blocks of 128 per SM that the register budgets of the u2p, radiative
+// viscosity, dynamo and boundary kernels must allow (1: uncapped). Measured on
+// the wedge: 3 (168 registers) makes u2p 5% and the dynamo 4% faster, and the
+// boundary kernel 3% slower; the viscosity kernel is indifferent.
+#ifndef KC_U2P_MIN_BLOCKS
+#define KC_U2P_MIN_BLOCKS 3
+#endif
+#ifndef KC_RIJVISC_MIN_BLOCKS
+#define KC_RIJVISC_MIN_BLOCKS 1
+#endif
+#ifndef KC_DYNAMO_MIN_BLOCKS
+#define KC_DYNAMO_MIN_BLOCKS 3
+#endif
+#ifndef KC_BC_MIN_BLOCKS
+#define KC_BC_MIN_BLOCKS 1
+#endif
+
 namespace kc {
 
 __device__ __forceinline__ void set_err(DevScalars* sc, int code, long long cell) {
@@ -246,7 +263,7 @@ __global__ void __launch_bounds__(128) k_update_entropy(DevState s, double gam) 
 }
 
 // ---- u2p (koral/sim.zig:924-1000) --------------------------------------------
-__global__ void __launch_bounds__(128) k_u2p(DevState s, DevScalars* sc, double gam, FloorParams fl, RadParams rp,
+__global__ void __launch_bounds__(128, KC_U2P_MIN_BLOCKS) k_u2p(DevState s, DevScalars* sc, double gam, FloorParams fl, RadParams rp,
                                              int polar_nc, int phi_fastest) {
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
@@ -474,7 +491,7 @@ struct BcArgs {
   double gam;
 };
 // ghost faces of one axis; thread t -> (ghost layer i, two transverse indices)
-__global__ void __launch_bounds__(128) k_bc_faces(DevState s, DevScalars* sc, BcArgs a, int axis) {
+__global__ void __launch_bounds__(128, KC_BC_MIN_BLOCKS) k_bc_faces(DevState s, DevScalars* sc, BcArgs a, int axis) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
   if (axis == 0) {
@@ -793,9 +810,14 @@ __device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, 
   }
   return E_OK;
 }
+#ifndef KC_FLUX_MIN_BLOCKS
+// resident blocks of 128 per SM the face kernel's register budget must allow:
+// 3 caps it at 168 registers (194 uncapped), measured 14% faster; 4 (128) 10%
+#define KC_FLUX_MIN_BLOCKS 3
+#endif
 // MIXED: the reconstruction and the LAXF combination in FP32 (kc_mixed.cuh)
 template <bool MIXED>
-__global__ void __launch_bounds__(128) k_face_flux(DevState s, DevScalars* sc, FluxArgs a, int dim) {
+__global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState s, DevScalars* sc, FluxArgs a, int dim) {
   long n = dim == 0 ? s.gr.nx : dim == 1 ? s.gr.ny : s.gr.nz;
   int c0d = dim == 0 ? 1 : 0, c1d = dim == 2 ? 1 : 2;
   long dims[3] = {s.gr.nx, s.gr.ny, s.gr.nz};
@@ -1202,7 +1224,7 @@ struct ViscArgs {
   int dt_slot;
   OpacParams op;
 };
-__global__ void __launch_bounds__(128) k_rijvisc(DevState s, ViscArgs a) {
+__global__ void __launch_bounds__(128, KC_RIJVISC_MIN_BLOCKS) k_rijvisc(DevState s, ViscArgs a) {
   const double dt = s.coef[a.dt_slot];
   long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
   Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};
@@ -1337,7 +1359,7 @@ struct DynArgs {
   int dt_slot;
   DynamoParams dp;
 };
-__global__ void __launch_bounds__(128) k_dynamo_delta_a(DevState s, DevScalars* sc, DynArgs a) {
+__global__ void __launch_bounds__(128, KC_DYNAMO_MIN_BLOCKS) k_dynamo_delta_a(DevState s, DevScalars* sc, DynArgs a) {
   const double dt = s.coef[a.dt_slot];
   long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
   Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};

@@ -392,8 +392,10 @@ void launch_implicit(kc_handle* h, int dt_slot) {
     x.guess = h->guess;
   }
   ++h->n_launch;
-  if (extra) k_implicit<true><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
-  else k_implicit<false><<<nblk(ndom, h->tpb_implicit), h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  unsigned nb = nblk(ndom, h->tpb_implicit);
+  if (extra) k_implicit<true, 2><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  else if (a.phi_fastest) k_implicit<false, 2><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  else k_implicit<false, 3><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
 }
 
 void launch_wavespeeds(kc_handle* h) {

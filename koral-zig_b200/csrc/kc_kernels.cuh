@@ -1020,15 +1020,13 @@ struct ImplExtra {
 };
 // EXTRA = false is the reference path alone (the guess and harvest code is not
 // compiled into it, so its registers and code size are those of the plain solve)
-// Resident blocks of 128 per SM that the implicit kernel's register budget must
-// allow: 3 caps it at 168 registers (12 warps per SM instead of 8); measured
-// 2-3% faster on the wedge than 255 registers, with 128 (4 blocks) in between.
-#ifndef KC_IMPLICIT_MIN_BLOCKS
-#define KC_IMPLICIT_MIN_BLOCKS 3
-#endif
-template <bool EXTRA>
-__global__ void __launch_bounds__(128, KC_IMPLICIT_MIN_BLOCKS) k_implicit(DevState s, DevScalars* sc, ImplArgs a,
-                                                                          ImplExtra x) {
+// MINB: resident blocks of 128 per SM that the register budget must allow.
+// With the x-fastest cell order (2D grids) 3 (168 registers, 12 warps per SM)
+// measured 2-3% faster than 255 registers (8 warps); with the phi-fastest order
+// of 3D grids, whose warps walk the solver together, 255 registers measured 6%
+// faster than 168 and 128 slower still. The host picks the instance by order.
+template <bool EXTRA, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* sc, ImplArgs a, ImplExtra x) {
   const double dt = s.coef[a.dt_slot];
   long ix, iy, iz;
   if (a.phi_fastest) {

@@ -1313,44 +1313,38 @@ __global__ void __launch_bounds__(128, KC_RIJVISC_MIN_BLOCKS) k_rijvisc(DevState
 }
 
 // ---- mimic dynamo (koral/sim/dynamo.zig) --------------------------------------
-// per-radius density-weighted scale height, the reference's iy-outer / iz-inner
-// accumulation order kept (one thread per radial column)
 // Per-radius scale height (dynamo.zig:158 calcScaleHeight). The fold over
 // (iy, iz) of each x column keeps the reference's serial order (iy outer, iz
-// inner), so it is one thread's job; a block serves 32 columns, its 8 warps
-// stage tiles of the fold's inputs in shared memory and lane ix of warp 0
-// folds them in order.
-constexpr int SH_COLS = 32, SH_WARPS = 8, SH_TILE = 48;
-__global__ void __launch_bounds__(256) k_scale_height(DevState s) {
-  __shared__ double t_rho[SH_TILE][SH_COLS], t_gd[SH_TILE][SH_COLS], t_th[SH_TILE][SH_COLS];
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  long ix = (long)blockIdx.x * SH_COLS + lane;
-  bool okx = ix < s.gr.nx;
+// inner). One warp per column: the lanes load and form 32 consecutive terms
+// (rho gdet and rho gdet dtheta^2) at a time, and every lane then folds those
+// 32 terms in order from shuffles, so the sums are the serial ones and the
+// loads of a chunk overlap; the columns run in parallel across the SMs.
+constexpr int SH_WARPS = 2;
+__global__ void __launch_bounds__(SH_WARPS * 32) k_scale_height(DevState s) {
+  const unsigned full = 0xffffffffu;
+  int lane = threadIdx.x & 31;
+  long ix = (long)blockIdx.x * SH_WARPS + (threadIdx.x >> 5);
+  if (ix >= s.gr.nx) return;  // whole warps leave together
   long nz = s.gr.nz, nsteps = (long)s.gr.ny * nz, nc = s.gr.nc;
   double sigma = 0.0, sth = 0.0;
-  for (long k0 = 0; k0 < nsteps; k0 += SH_TILE) {
-    for (int j = warp; j < SH_TILE; j += SH_WARPS) {
-      long k = k0 + j;
-      if (k < nsteps && okx) {
-        long c = cidx(s.gr, ix, k / nz, k % nz);
-        t_rho[j][lane] = s.p[RHO * nc + c];
-        t_gd[j][lane] = s.cgc[10L * nc + c];
-        t_th[j][lane] = s.blg[27L * nc + c];
-      }
+  for (long k0 = 0; k0 < nsteps; k0 += 32) {
+    long k = k0 + lane;
+    double a = 0.0, b = 0.0;
+    if (k < nsteps) {
+      long c = cidx(s.gr, ix, k / nz, k % nz);
+      double rho = s.p[RHO * nc + c], gd = s.cgc[10L * nc + c];
+      double dth = KP_PI / 2.0 - s.blg[27L * nc + c];
+      a = rho * gd;
+      b = rho * gd * dth * dth;
     }
-    __syncthreads();
-    if (warp == 0 && okx) {
-      long m = nsteps - k0 < SH_TILE ? nsteps - k0 : SH_TILE;
-      for (int j = 0; j < m; ++j) {
-        double rho = t_rho[j][lane], gd = t_gd[j][lane];
-        double dth = KP_PI / 2.0 - t_th[j][lane];
-        sigma += rho * gd;
-        sth += rho * gd * dth * dth;
-      }
+    int m = nsteps - k0 < 32 ? (int)(nsteps - k0) : 32;
+    for (int j = 0; j < m; ++j) {
+      double aj = __shfl_sync(full, a, j), bj = __shfl_sync(full, b, j);
+      sigma += aj;
+      sth += bj;
     }
-    __syncthreads();
   }
-  if (warp == 0 && okx) s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
+  if (lane == 0) s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
 }
 struct DynArgs {
   double gam, a, rhor, risco;

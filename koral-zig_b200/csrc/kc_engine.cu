@@ -284,12 +284,14 @@ void launch_set_bc(kc_handle* h) {
     k_corners_2d<<<1, 32, 0, st>>>(h->ds, a);
   } else if (gr.nz > 1 && gr.ny > 1) {
     long ng = gr.ng;
-    ++h->n_launch;
-    k_edge_tubes<<<nblk(4L * (gr.nz + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 0, 1, 2);
-    ++h->n_launch;
-    k_edge_tubes<<<nblk(4L * (gr.ny + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 0, 2, 1);
-    ++h->n_launch;
-    k_edge_tubes<<<nblk(4L * (gr.nx + 2 * ng)), TPB, 0, st>>>(h->ds, a.gam, 1, 2, 0);
+    const int planes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+    long nt0 = 2 * (ng - 1) + 1;
+    for (const auto& pl : planes) {
+      long nslice = (pl[2] == 0 ? gr.nx : pl[2] == 1 ? gr.ny : gr.nz) + 2 * ng;
+      h->n_launch += 2;
+      k_edge_tubes<<<nblk(4L * nslice * nt0, 64), 64, 0, st>>>(h->ds, a.gam, pl[0], pl[1], pl[2], 0);
+      k_edge_tubes<<<nblk(4L * nslice, 64), 64, 0, st>>>(h->ds, a.gam, pl[0], pl[1], pl[2], 1);
+    }
     ++h->n_launch;
     k_corner_cubes<<<nblk(ng * ng * ng), TPB, 0, st>>>(h->ds, a.gam);
   }

@@ -602,48 +602,55 @@ __global__ void k_corners_2d(DevState s, BcArgs a) {
 }
 
 // one group of four 3D edge tubes (bc.zig:404): thread -> (tube, slice)
-__global__ void k_edge_tubes(DevState s, double gam, int pa, int pb, int pc) {
+// The four edge tubes of the (pa, pb) plane along pc (bc.zig:420), in two
+// phases. Phase 0: per (tube, cc), the 2 (ng-1) copies from the face ghosts and
+// the (g1, g1) average, all independent (each writes its own cell and reads
+// face ghosts only), one thread each. Phase 1: the (g2, g2) average, which
+// reads two cells phase 0 wrote. Same values as one thread doing them in order.
+__device__ __forceinline__ void tube_cell(int pa, int pb, int pc, long av, long bv, long cv, long o[3]) {
+  o[pa] = av;
+  o[pb] = bv;
+  o[pc] = cv;
+}
+__global__ void k_edge_tubes(DevState s, double gam, int pa, int pb, int pc, int phase) {
   long dims[3] = {s.gr.nx, s.gr.ny, s.gr.nz};
   long ng = s.gr.ng;
   long nslice = dims[pc] + 2 * ng;
+  long ntask = phase == 0 ? 2 * (ng - 1) + 1 : 1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 4 * nslice) return;
-  int tube = (int)(t / nslice);
-  long cc = -ng + t % nslice;
+  if (t >= 4 * nslice * ntask) return;
+  long task = t % ntask, q = t / ntask;
+  int tube = (int)(q / nslice);
+  long cc = -ng + q % nslice;
   bool a_hi = tube & 2, b_hi = tube & 1;
   long na = dims[pa], nb = dims[pb];
   long a_edge = a_hi ? na - 1 : 0, a_g1 = a_hi ? na : -1, a_g2 = a_hi ? na + 1 : -2;
   long b_edge = b_hi ? nb - 1 : 0, b_g1 = b_hi ? nb : -1, b_g2 = b_hi ? nb + 1 : -2;
-  auto cell = [&](long av, long bv, long cv, long o[3]) {
-    o[pa] = av;
-    o[pb] = bv;
-    o[pc] = cv;
-  };
-  for (long i = 0; i < ng - 1; ++i) {
+  long d[3], x[3], y[3];
+  if (phase == 1) {
+    tube_cell(pa, pb, pc, a_g2, b_g2, cc, d);
+    tube_cell(pa, pb, pc, a_g2, b_g1, cc, x);
+    tube_cell(pa, pb, pc, a_g1, b_g2, cc, y);
+    avg_p_cell(s, d, x, y);
+  } else if (task == 2 * (ng - 1)) {
+    tube_cell(pa, pb, pc, a_g1, b_g1, cc, d);
+    tube_cell(pa, pb, pc, a_g1, b_edge, cc, x);
+    tube_cell(pa, pb, pc, a_edge, b_g1, cc, y);
+    avg_p_cell(s, d, x, y);
+  } else {
+    long i = task >> 1;
     long a_out = a_hi ? na + i + 1 : -ng + i;
     long b_out = b_hi ? nb + i + 1 : -ng + i;
-    long d[3], src[3];
-    cell(a_out, b_g1, cc, d);
-    cell(a_out, b_edge, cc, src);
-    copy_p_cell(s, d[0], d[1], d[2], src[0], src[1], src[2]);
-    p2u_cell(s, d[0], d[1], d[2], gam);
-    cell(a_g1, b_out, cc, d);
-    cell(a_edge, b_out, cc, src);
-    copy_p_cell(s, d[0], d[1], d[2], src[0], src[1], src[2]);
-    p2u_cell(s, d[0], d[1], d[2], gam);
+    if ((task & 1) == 0) {
+      tube_cell(pa, pb, pc, a_out, b_g1, cc, d);
+      tube_cell(pa, pb, pc, a_out, b_edge, cc, x);
+    } else {
+      tube_cell(pa, pb, pc, a_g1, b_out, cc, d);
+      tube_cell(pa, pb, pc, a_edge, b_out, cc, x);
+    }
+    copy_p_cell(s, d[0], d[1], d[2], x[0], x[1], x[2]);
   }
-  long d1[3], x1[3], y1[3];
-  cell(a_g1, b_g1, cc, d1);
-  cell(a_g1, b_edge, cc, x1);
-  cell(a_edge, b_g1, cc, y1);
-  avg_p_cell(s, d1, x1, y1);
-  p2u_cell(s, d1[0], d1[1], d1[2], gam);
-  long d2[3], x2[3], y2[3];
-  cell(a_g2, b_g2, cc, d2);
-  cell(a_g2, b_g1, cc, x2);
-  cell(a_g1, b_g2, cc, y2);
-  avg_p_cell(s, d2, x2, y2);
-  p2u_cell(s, d2[0], d2[1], d2[2], gam);
+  p2u_cell(s, d[0], d[1], d[2], gam);
 }
 // the 8 corner cubes (bc.zig:457), in the reference's cube order
 __global__ void k_corner_cubes(DevState s, double gam) {

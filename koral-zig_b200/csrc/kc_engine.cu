@@ -293,7 +293,7 @@ void launch_set_bc(kc_handle* h) {
       k_edge_tubes<<<nblk(4L * nslice, 64), 64, 0, st>>>(h->ds, a.gam, pl[0], pl[1], pl[2], 1);
     }
     ++h->n_launch;
-    k_corner_cubes<<<nblk(ng * ng * ng), TPB, 0, st>>>(h->ds, a.gam);
+    k_corner_cubes<<<nblk(8 * ng * ng * ng, 64), 64, 0, st>>>(h->ds, a.gam);
   }
 }
 

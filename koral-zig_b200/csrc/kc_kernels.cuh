@@ -652,19 +652,21 @@ __global__ void k_edge_tubes(DevState s, double gam, int pa, int pb, int pc, int
   }
   p2u_cell(s, d[0], d[1], d[2], gam);
 }
-// the 8 corner cubes (bc.zig:457), in the reference's cube order
+// the 8 corner cubes (bc.zig:457)
+// Every cube cell copies its cube's domain corner cell, which no cube writes,
+// so the 8 x ng^3 cells are independent: one thread each.
 __global__ void k_corner_cubes(DevState s, double gam) {
   long ng = s.gr.ng;
   long per = ng * ng * ng;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= per) return;
+  if (t >= 8 * per) return;
+  int cube = (int)(t / per);
+  t %= per;
   long nx = s.gr.nx, ny = s.gr.ny, nz = s.gr.nz;
-  for (int cube = 0; cube < 8; ++cube) {
-    bool xh = cube & 1, yh = cube & 2, zh = cube & 4;
-    long ix = (xh ? nx : -ng) + t % ng, iy = (yh ? ny : -ng) + (t / ng) % ng, iz = (zh ? nz : -ng) + t / (ng * ng);
-    copy_p_cell(s, ix, iy, iz, xh ? nx - 1 : 0, yh ? ny - 1 : 0, zh ? nz - 1 : 0);
-    p2u_cell(s, ix, iy, iz, gam);
-  }
+  bool xh = cube & 1, yh = cube & 2, zh = cube & 4;
+  long ix = (xh ? nx : -ng) + t % ng, iy = (yh ? ny : -ng) + (t / ng) % ng, iz = (zh ? nz : -ng) + t / (ng * ng);
+  copy_p_cell(s, ix, iy, iz, xh ? nx - 1 : 0, yh ? ny - 1 : 0, zh ? nz - 1 : 0);
+  p2u_cell(s, ix, iy, iz, gam);
 }
 
 // ---- polar axis overwrite (koral/sim/polaraxis.zig:124) -----------------------

@@ -240,10 +240,11 @@ int kc_set_graph(kc_handle* h, int32_t on);
 
 /* The autotuner's choice (no reference counterpart): implicit form
  * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT), threads per block of the
- * per-cell implicit, face-flux and u2p kernels, and on 3D grids the per-cell
- * implicit kernel's thread -> cell order (1: phi fastest, the default, so that
- * a warp's cells share r and theta; 0: x fastest), with the measured step time
- * of the choice and of the configuration on entry. */
+ * per-cell implicit, face-flux and u2p kernels, and the per-cell implicit
+ * kernel's thread -> cell order (1, the default: phi fastest on 3D grids, so
+ * that a warp's cells share r and theta, theta fastest on 2D grids; 0: x
+ * fastest), with the measured step time of the choice and of the
+ * configuration on entry. */
 typedef struct kc_tune_result {
   int32_t implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
   double ms_per_step, ms_per_step_entry;

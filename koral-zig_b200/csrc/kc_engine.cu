@@ -70,8 +70,9 @@ struct kc_handle {
 #ifndef KC_U2P_PHI_FASTEST
 #define KC_U2P_PHI_FASTEST 0
 #endif
-  // thread -> cell order of the per-cell implicit and u2p kernels on 3D grids:
-  // phi fastest (warps of cells sharing r and theta) or x fastest
+  // thread -> cell order of the per-cell implicit and u2p kernels: on 3D grids
+  // phi fastest (warps of cells sharing r and theta) or x fastest; for the
+  // implicit kernel on 2D grids the same switch selects theta fastest
   int implicit_phi_fastest = KC_IMPLICIT_PHI_FASTEST, u2p_phi_fastest = KC_U2P_PHI_FASTEST;
   // the step's dt-derived coefficients: pinned host table and its device copy
   // (DevState::coef); slots 0-3 are fixed by run_step, later ones appended
@@ -335,6 +336,7 @@ void launch_implicit(kc_handle* h, int dt_slot) {
   a.ip = h->sp.ip;
   a.polar_nc = h->sp.correct_polaraxis ? h->sp.nccorrectpolar : 0;
   a.phi_fastest = h->implicit_phi_fastest && gr.nz > 1;
+  a.y_fastest = h->implicit_phi_fastest && gr.nz == 1;
   PassScope ps(h, KC_PASS_IMPLICIT);
   // the learned guess and the harvest run in the per-cell form
   bool extra = h->guess_mode == KC_GUESS_MLP || h->hcap > 0;
@@ -1957,8 +1959,9 @@ void tune_restore(kc_handle* h, const TuneSnapshot& sn) {
 }  // namespace
 
 // Picks the implicit form (per-cell or split), the block sizes of the
-// per-cell implicit, face-flux and u2p kernels and (3D) the per-cell implicit
-// kernel's cell order (phi or x fastest) by timing whole steps on the
+// per-cell implicit, face-flux and u2p kernels and the per-cell implicit
+// kernel's cell order (phi on 3D or theta on 2D fastest, or x fastest) by
+// timing whole steps on the
 // handle's current state, one knob at a time (coordinate descent from the
 // configuration on entry). Each trial restores the state, runs one untimed step
 // (with the graph form on, a second one, so the timed steps replay the graph)
@@ -2012,7 +2015,6 @@ extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
   const int forms[2] = {KC_IMPLICIT_PER_CELL, KC_IMPLICIT_SPLIT};
   const int sizes[3] = {64, 96, 128};
   for (int knob = 0; knob < 5 && !st; ++knob) {
-    if (knob == 4 && h->gr.nz == 1) break;  // the cell order matters on 3D grids only
     int n = (knob == 0 || knob == 4) ? 2 : 3;
     for (int i = 0; i < n && !st; ++i) {
       TuneConfig c = best;

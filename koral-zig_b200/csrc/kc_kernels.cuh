@@ -1013,6 +1013,7 @@ struct ImplArgs {
   double gam;
   int dt_slot;  // the pass's dt in DevState::coef
   int phi_fastest;  // thread -> cell order of the per-cell kernel: 1 = phi fastest, 0 = x fastest
+  int y_fastest;    // without phi_fastest: theta (y) fastest instead of x (2D grids)
   RadParams rp;
   OpacParams op;
   ImplicitParams ip;
@@ -1040,6 +1041,15 @@ __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* 
   long ix, iy, iz;
   if (a.phi_fastest) {
     if (!domain_cell_phi_fastest(s.gr, ix, iy, iz)) return;
+  } else if (a.y_fastest) {
+    // 2D: neighbours in theta at one radius (measured 10% faster than x fastest
+    // on the 384x360 grid; 8 x 4 tiles per warp were in between)
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)s.gr.nx * s.gr.ny * s.gr.nz) return;
+    iy = t % s.gr.ny;
+    long q = t / s.gr.ny;
+    ix = q % s.gr.nx;
+    iz = q / s.gr.nx;
   } else {
     Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
     if (!range_cell(r, ix, iy, iz)) return;

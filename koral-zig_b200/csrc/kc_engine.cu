@@ -434,8 +434,18 @@ void launch_face_fluxes(kc_handle* h) {
     long n = (dims[dim] + 1) * n0 * n1;
     ++h->n_launch;
     int tb = h->tpb_flux;
-    if (h->opt.precision == KC_MIXED) k_face_flux<true><<<nblk(n, tb), tb, 0, h->stream>>>(h->ds, h->dsc, a, dim);
-    else k_face_flux<false><<<nblk(n, tb), tb, 0, h->stream>>>(h->ds, h->dsc, a, dim);
+    unsigned nb = nblk(n, tb);
+    bool mx = h->opt.precision == KC_MIXED;
+    if (dim == 0) {
+      if (mx) k_face_flux<true, 0><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+      else k_face_flux<false, 0><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+    } else if (dim == 1) {
+      if (mx) k_face_flux<true, 1><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+      else k_face_flux<false, 1><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+    } else {
+      if (mx) k_face_flux<true, 2><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+      else k_face_flux<false, 2><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+    }
   }
 }
 

@@ -825,8 +825,11 @@ __device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, 
 #define KC_FLUX_MIN_BLOCKS 3
 #endif
 // MIXED: the reconstruction and the LAXF combination in FP32 (kc_mixed.cuh)
-template <bool MIXED>
-__global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState s, DevScalars* sc, FluxArgs a, int dim) {
+// DIM: the face direction, a template argument so that every index along it
+// is a compile-time one (one instance per direction)
+template <bool MIXED, int DIM>
+__global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState s, DevScalars* sc, FluxArgs a) {
+  constexpr int dim = DIM;
   long n = dim == 0 ? s.gr.nx : dim == 1 ? s.gr.ny : s.gr.nz;
   int c0d = dim == 0 ? 1 : 0, c1d = dim == 2 ? 1 : 2;
   long dims[3] = {s.gr.nx, s.gr.ny, s.gr.nz};

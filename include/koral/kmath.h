@@ -106,10 +106,13 @@ KC_HD double fabs(double x) { return from_bits(to_bits(x) & 0x7fffffffffffffffUL
 KC_HD double copysign(double x, double s) {
   return from_bits((to_bits(x) & 0x7fffffffffffffffULL) | (to_bits(s) & 0x8000000000000000ULL));
 }
-// Out of line on the device (one copy of the IEEE square-root sequence per
-// kernel instead of one per call site): the solver kernels are bound by
-// instruction fetch, and their code size is what matters there.
-KC_HDN double sqrt(double x) {
+// Inline: out of line (one copy of the IEEE square-root sequence per kernel)
+// was measured 1% slower once the implicit kernel's warps became coherent
+// (the phi-fastest cell order); KC_SQRT_ATTR=KC_HDN selects it.
+#ifndef KC_SQRT_ATTR
+#define KC_SQRT_ATTR KC_HD
+#endif
+KC_SQRT_ATTR double sqrt(double x) {
 #if defined(__CUDA_ARCH__)
   return __dsqrt_rn(x);
 #else
@@ -122,7 +125,10 @@ KC_HDN double sqrt(double x) {
 // is far larger than the instruction cache), and an inline double divide is
 // ~30 instructions at every site. The result is the same correctly rounded
 // quotient as `a / b`.
-KC_HDN double div(double a, double b) { return a / b; }
+#ifndef KC_DIV_ATTR
+#define KC_DIV_ATTR KC_HDN
+#endif
+KC_DIV_ATTR double div(double a, double b) { return a / b; }
 // Zig's @min/@max on floats: the non-NaN operand wins (LLVM minnum/maxnum).
 KC_HD double fmin(double a, double b) {
   if (a != a) return b;

@@ -202,7 +202,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2}
+IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2, "sorted": 3}
 IMPL_METRIC = "implicit M1 solves/s (batched, independent cells)"
 IMPL_UNIT = "solves/s"
 
@@ -485,10 +485,13 @@ def main():
     ap.add_argument("--pairs", type=int, default=1000000, help="training pairs of the guess workload")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
-    ap.add_argument("--implicit-mode", default="per-cell", choices=["per-cell", "compacting", "split"],
-                    help="implicit solve form: one thread per cell, the persistent lane-refilling state machine, or the "
-                         "split opening + compacted-ladder pair")
+    ap.add_argument("--implicit-mode", default=None, choices=["per-cell", "compacting", "split", "sorted"],
+                    help="implicit solve form: one thread per cell, the persistent lane-refilling state machine, the "
+                         "split opening + compacted-ladder pair, or (batch workload only) the per-cell kernel over "
+                         "key-sorted cells; default: sorted for --workload implicit, per-cell otherwise")
     args = ap.parse_args()
+    if args.implicit_mode is None:  # sorted is a batch form; the step's default form is per-cell
+        args.implicit_mode = "sorted" if args.workload == "implicit" else "per-cell"
     if args.steps is None:
         args.steps = 3 if args.workload == "implicit" else 20
     rank = int(os.environ.get("RANK", 0))

@@ -56,8 +56,9 @@ enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
  * PER_CELL one thread per cell; COMPACTING a persistent lane-refilling state
  * machine; SPLIT an opening kernel that finishes every cell passing the Newton
  * core's first residual test at its warm start and a ladder kernel over the
- * compacted rest */
-enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1, KC_IMPLICIT_SPLIT = 2 };
+ * compacted rest; SORTED (the batch entry points only) the per-cell kernel over
+ * the cells sorted by start fluid, optical depth and temperature */
+enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1, KC_IMPLICIT_SPLIT = 2, KC_IMPLICIT_SORTED = 3 };
 
 /* Pass ids of the per-pass timers, the members of koral/sim/timers.zig:4
  * Pass that the device step has. KC_PASS_FLUXES covers the reference's

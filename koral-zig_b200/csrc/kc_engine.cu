@@ -14,6 +14,8 @@
 #include <thread>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "kc_kernels.cuh"
 #include "../../include/koral/kdump.h"
 #include "../../include/koral/kinit.h"
@@ -1399,9 +1401,10 @@ struct BatchArgs {
 
 __global__ void __launch_bounds__(128) k_implicit_batch(long n, const double* __restrict__ geom23,
                                                         const double* __restrict__ dt, double* pp_io, int* res,
-                                                        BatchArgs a) {
-  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                                                        BatchArgs a, const int* order = nullptr) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  long i = order ? order[t] : t;  // the sorted form visits cells in key order
   Geom g;
   geom_from_record23(geom23 + i * 23, g);
   double pp[NV], uu[NV];
@@ -1481,13 +1484,56 @@ __global__ void __launch_bounds__(128) k_implicit_batch_persistent(long n, const
   ImpParams P{a.gam, a.rp, a.op, a.ip};
   imp_persistent(src, n, counter, P);
 }
-// launch either form of the batch on `st`; the persistent form takes a
-// zeroed counter from the stream-ordered allocator
+// Sort key of a batch cell for the sorted form: the start fluid of the solve
+// (the ladder's first branch), then the cell's optical-depth proxy log10(rho dt)
+// and its temperature proxy log10(u / rho), each quantised to 1/8 decade, so
+// that a warp's lanes get cells that take similar paths through the solver.
+__global__ void k_batch_key(long n, const double* __restrict__ geom23, const double* __restrict__ dt,
+                            const double* __restrict__ pp_in, BatchArgs a, unsigned* key, int* idx) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Geom g;
+  geom_from_record23(geom23 + i * 23, g);
+  double pp[NV];
+  for (int k = 0; k < NV; ++k) pp[k] = pp_in[i * NV + k];
+  double ehat = -calc_ff_rtt(pp, g, nullptr);
+  unsigned start = (ehat < a.ip.threshold * pp[UU]) ? 1u : 0u;
+  auto q = [](double x, double lo) -> unsigned {  // 1/8-decade bins over 128 decades
+    double b = (::log10(x) - lo) * 8.0;
+    return (b > 0.0 && b < 1023.0) ? (unsigned)b : (b >= 1023.0 ? 1023u : 0u);
+  };
+  key[i] = (start << 20) | (q(pp[RHO] * dt[i], -64.0) << 10) | q(pp[UU] / pp[RHO], -64.0);
+  idx[i] = (int)i;
+}
+// launch either form of the batch on `st`; the persistent and sorted forms take
+// their scratch from the stream-ordered allocator
 int launch_batch(long n, const double* g, const double* d, double* p, int* r, const BatchArgs& a, int mode,
                  cudaStream_t st) {
   if (mode == KC_IMPLICIT_PER_CELL) {
     k_implicit_batch<<<nblk(n), TPB, 0, st>>>(n, g, d, p, r, a);
     return cudaGetLastError() == cudaSuccess ? KC_OK : KC_ERR_CUDA;
+  }
+  if (mode == KC_IMPLICIT_SORTED) {
+    if (n > 0x7fffffffL) return KC_ERR_INVALID_CONFIG;
+    unsigned *k0 = nullptr, *k1 = nullptr;
+    int *i0 = nullptr, *i1 = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, i0, i1, (int)n, 0, 21, st);
+    if (cudaMallocAsync((void**)&k0, n * 4, st) != cudaSuccess || cudaMallocAsync((void**)&k1, n * 4, st) != cudaSuccess ||
+        cudaMallocAsync((void**)&i0, n * 4, st) != cudaSuccess || cudaMallocAsync((void**)&i1, n * 4, st) != cudaSuccess ||
+        cudaMallocAsync(&tmp, tmp_bytes, st) != cudaSuccess)
+      return KC_ERR_OOM;
+    k_batch_key<<<nblk(n), TPB, 0, st>>>(n, g, d, p, a, k0, i0);
+    cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, i0, i1, (int)n, 0, 21, st);
+    k_implicit_batch<<<nblk(n), TPB, 0, st>>>(n, g, d, p, r, a, i1);
+    cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(tmp, st);
+    cudaFreeAsync(k0, st);
+    cudaFreeAsync(k1, st);
+    cudaFreeAsync(i0, st);
+    cudaFreeAsync(i1, st);
+    return e == cudaSuccess ? KC_OK : KC_ERR_CUDA;
   }
   if (mode != KC_IMPLICIT_COMPACTING) return KC_ERR_INVALID_CONFIG;
   int dev = 0, nsm = 0, per_sm = 0;
@@ -1533,7 +1579,8 @@ extern "C" int kc_implicit_batch(const kc_options* opt, int64_t n, const double*
   BatchArgs a;
   int st = batch_prepare(opt, a);
   if (st) return st;
-  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING) return KC_ERR_INVALID_CONFIG;
+  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING && mode != KC_IMPLICIT_SORTED)
+    return KC_ERR_INVALID_CONFIG;
   if (n <= 0) return KC_OK;
   DevBuf dg, dd, dp, dr;
   if (cudaMalloc(&dg.p, n * 23 * 8) || cudaMalloc(&dd.p, n * 8) || cudaMalloc(&dp.p, n * NV * 8) ||

@@ -22,7 +22,7 @@ KC_OK = 0
 KC_ERR_INVALID_CONFIG = 1
 KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
-KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT = 0, 1, 2
+KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT, KC_IMPLICIT_SORTED = 0, 1, 2, 3
 KC_NPASS = 14
 KC_ERR_TOO_MANY_CELLS = 9
 KC_NOALLOC_MAX_CELLS = 16384

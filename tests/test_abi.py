@@ -77,3 +77,40 @@ def test_create_without_a_device_fails_loudly():
     kc = koralcuda()
     with pytest.raises(kc.KoralError):
         kc.Sim(kc.puffy_grid(32, 30), kc.puffy_options())
+
+
+STRUCTS = {"kc_grid": "KcGrid", "kc_options": "KcOptions", "kc_counters": "KcCounters",
+           "kc_step_info": "KcStepInfo", "kc_scalar_row": "KcScalarRow", "kc_tune_result": "KcTuneResult",
+           "kc_dump_header": "KcDumpHeader"}
+
+
+def test_ctypes_mirror_matches_header_layouts(tmp_path):
+    """Every POD struct of the header has the same size and field offsets in the
+    Python mirror (a C program built here prints them from the header itself)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    kc = koralcuda()
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "koralcuda.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(kc, pyname)._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            name, field, val = ln.split()
+            got[(name, field)] = int(val)
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(kc, pyname)
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)

@@ -158,7 +158,7 @@ T* dalloc(kc_handle* h, size_t n, int& st) {
   return (T*)p;
 }
 
-// ---- metric cache, host-built once (koral/metric/precompute.zig:175) ----------
+// ---- metric cache, built once on the device (koral/metric/precompute.zig:175) ---
 int build_cache(kc_handle* h) {
   const Grid& g = h->gr.g;
   long nc = h->gr.nc, sx = h->gr.sx, sy = h->gr.sy, sz = h->gr.sz;
@@ -1365,827 +1365,8 @@ int kc_init_puffy(kc_handle* h, double perturb, double perturb_rho, uint64_t see
 
 }  // extern "C"
 
-// ==== batched per-cell entry points ============================================
-namespace {
-
-// golden-record geometry: gg and GG upper triangles, gdet, alpha, gttpert
-// (koral/testing/golden.zig:241 geomFromRecord)
-__device__ void geom_from_record23(const double* v, Geom& g) {
-  for (int i = 0; i < 4; ++i)
-    for (int j = 0; j < 5; ++j) {
-      g.gg[i][j] = 0.0;
-      g.GG[i][j] = 0.0;
-    }
-  int n = 0;
-  for (int i = 0; i < 4; ++i)
-    for (int j = i; j < 4; ++j) {
-      g.gg[i][j] = v[n];
-      g.gg[j][i] = v[n];
-      g.GG[i][j] = v[10 + n];
-      g.GG[j][i] = v[10 + n];
-      ++n;
-    }
-  g.gdet = v[20];
-  g.alpha = v[21];
-  g.gttpert = v[22];
-  for (int i = 0; i < 4; ++i) g.xx[i] = 0.0;
-}
-
-struct BatchArgs {
-  double gam;
-  RadParams rp;
-  OpacParams op;
-  ImplicitParams ip;
-  FloorParams fl;
-};
-
-__global__ void __launch_bounds__(128) k_implicit_batch(long n, const double* __restrict__ geom23,
-                                                        const double* __restrict__ dt, double* pp_io, int* res,
-                                                        BatchArgs a, const int* order = nullptr) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  long i = order ? order[t] : t;  // the sorted form visits cells in key order
-  Geom g;
-  geom_from_record23(geom23 + i * 23, g);
-  double pp[NV], uu[NV];
-  for (int k = 0; k < NV; ++k) pp[k] = pp_io[i * NV + k];
-  ImplicitResult r = solve_implicit_lab(uu, pp, g, dt[i], a.gam, a.rp, a.op, a.ip);
-  for (int k = 0; k < NV; ++k) pp_io[i * NV + k] = pp[k];
-  int* o = res + i * 6;
-  o[0] = r.ok;
-  o[1] = r.rung;
-  o[2] = r.iters;
-  o[3] = r.whichprim;
-  o[4] = r.whicheq;
-  o[5] = r.whichframe;
-}
-
-__global__ void __launch_bounds__(128) k_u2p_batch(long n, const double* __restrict__ geom23,
-                                                   const double* __restrict__ uu_in, double* pp_io, int* fl_out,
-                                                   BatchArgs a) {
-  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  Geom g;
-  geom_from_record23(geom23 + i * 23, g);
-  double pp[NV], uu[NV];
-  for (int k = 0; k < NV; ++k) {
-    pp[k] = pp_io[i * NV + k];
-    uu[k] = uu_in[i * NV + k];
-  }
-  U2pMhdRes res = u2p_mhd(uu, pp, g, a.gam, a.fl);
-  U2pRadRes rr = u2p_rad(uu, pp, g, a.rp);
-  int gc = 0;
-  check_floors_mhd(pp, g, a.gam, a.fl, gc);
-  check_floors_rad(pp, g, a.rp);
-  for (int k = 0; k < NV; ++k) pp_io[i * NV + k] = pp[k];
-  fl_out[i * 3 + 0] = res.entropy_used;
-  fl_out[i * 3 + 1] = res.fixup;
-  fl_out[i * 3 + 2] = rr.corrected ? -1 : 0;
-}
-
-// the batch as a persistent, lane-refilling solve (kc_implicit_sm.cuh)
-struct ImpBatchSrc {
-  const double* geom23;
-  const double* dt;
-  double* pp_io;
-  int* res;
-  __device__ bool load(long i, ImpLane& L) {
-    geom_from_record23(geom23 + i * 23, L.g);
-    for (int k = 0; k < NV; ++k) L.pp00[k] = pp_io[i * NV + k];
-    L.dt = dt[i];
-    L.cell = i;
-    return true;
-  }
-  __device__ void store(const ImpLane& L) {
-    long i = L.cell;
-    int* o = res + i * 6;
-    if (L.ok) {
-      for (int k = 0; k < NV; ++k) pp_io[i * NV + k] = L.pp[k];
-      o[0] = 1;
-      o[1] = L.rung;
-      o[2] = L.iters;
-      o[3] = L.p;
-      o[4] = L.e;
-      o[5] = L.fr;
-    } else {
-      o[0] = 0;
-      o[1] = -1;
-      o[2] = 0;
-      o[3] = PRIM_RAD;
-      o[4] = EQ_ENERGY;
-      o[5] = FRAME_LAB;
-    }
-  }
-};
-__global__ void __launch_bounds__(128) k_implicit_batch_persistent(long n, const double* geom23, const double* dt,
-                                                                   double* pp_io, int* res, BatchArgs a,
-                                                                   unsigned long long* counter) {
-  ImpBatchSrc src{geom23, dt, pp_io, res};
-  ImpParams P{a.gam, a.rp, a.op, a.ip};
-  imp_persistent(src, n, counter, P);
-}
-// Sort key of a batch cell for the sorted form: the start fluid of the solve
-// (the ladder's first branch), then the cell's optical-depth proxy log10(rho dt)
-// and its temperature proxy log10(u / rho), each quantised to 1/8 decade, so
-// that a warp's lanes get cells that take similar paths through the solver.
-__global__ void k_batch_key(long n, const double* __restrict__ geom23, const double* __restrict__ dt,
-                            const double* __restrict__ pp_in, BatchArgs a, unsigned* key, int* idx) {
-  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  Geom g;
-  geom_from_record23(geom23 + i * 23, g);
-  double pp[NV];
-  for (int k = 0; k < NV; ++k) pp[k] = pp_in[i * NV + k];
-  double ehat = -calc_ff_rtt(pp, g, nullptr);
-  unsigned start = (ehat < a.ip.threshold * pp[UU]) ? 1u : 0u;
-  auto q = [](double x, double lo) -> unsigned {  // 1/8-decade bins over 128 decades
-    double b = (::log10(x) - lo) * 8.0;
-    return (b > 0.0 && b < 1023.0) ? (unsigned)b : (b >= 1023.0 ? 1023u : 0u);
-  };
-  key[i] = (start << 20) | (q(pp[RHO] * dt[i], -64.0) << 10) | q(pp[UU] / pp[RHO], -64.0);
-  idx[i] = (int)i;
-}
-// launch either form of the batch on `st`; the persistent and sorted forms take
-// their scratch from the stream-ordered allocator
-int launch_batch(long n, const double* g, const double* d, double* p, int* r, const BatchArgs& a, int mode,
-                 cudaStream_t st) {
-  if (mode == KC_IMPLICIT_PER_CELL) {
-    k_implicit_batch<<<nblk(n), TPB, 0, st>>>(n, g, d, p, r, a);
-    return cudaGetLastError() == cudaSuccess ? KC_OK : KC_ERR_CUDA;
-  }
-  if (mode == KC_IMPLICIT_SORTED) {
-    if (n > 0x7fffffffL) return KC_ERR_INVALID_CONFIG;
-    unsigned *k0 = nullptr, *k1 = nullptr;
-    int *i0 = nullptr, *i1 = nullptr;
-    void* tmp = nullptr;
-    size_t tmp_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, i0, i1, (int)n, 0, 21, st);
-    if (cudaMallocAsync((void**)&k0, n * 4, st) != cudaSuccess || cudaMallocAsync((void**)&k1, n * 4, st) != cudaSuccess ||
-        cudaMallocAsync((void**)&i0, n * 4, st) != cudaSuccess || cudaMallocAsync((void**)&i1, n * 4, st) != cudaSuccess ||
-        cudaMallocAsync(&tmp, tmp_bytes, st) != cudaSuccess)
-      return KC_ERR_OOM;
-    k_batch_key<<<nblk(n), TPB, 0, st>>>(n, g, d, p, a, k0, i0);
-    cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, i0, i1, (int)n, 0, 21, st);
-    k_implicit_batch<<<nblk(n), TPB, 0, st>>>(n, g, d, p, r, a, i1);
-    cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(tmp, st);
-    cudaFreeAsync(k0, st);
-    cudaFreeAsync(k1, st);
-    cudaFreeAsync(i0, st);
-    cudaFreeAsync(i1, st);
-    return e == cudaSuccess ? KC_OK : KC_ERR_CUDA;
-  }
-  if (mode != KC_IMPLICIT_COMPACTING) return KC_ERR_INVALID_CONFIG;
-  int dev = 0, nsm = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_implicit_batch_persistent, TPB, 0);
-  long need = (n + TPB - 1) / TPB, cap = (long)(per_sm > 0 ? per_sm : 1) * (nsm > 0 ? nsm : 1);
-  void* counter = nullptr;
-  if (cudaMallocAsync(&counter, sizeof(unsigned long long), st) != cudaSuccess) return KC_ERR_OOM;
-  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
-  k_implicit_batch_persistent<<<(unsigned)(need < cap ? need : cap), TPB, 0, st>>>(n, g, d, p, r, a,
-                                                                                   (unsigned long long*)counter);
-  cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(counter, st);
-  return e == cudaSuccess ? KC_OK : KC_ERR_CUDA;
-}
-
-struct DevBuf {
-  void* p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-};
-int batch_prepare(const kc_options* opt, BatchArgs& a) {
-  if (!opt || opt->abi_version != KC_ABI_VERSION) return KC_ERR_INVALID_CONFIG;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return KC_ERR_NO_DEVICE;
-  if (cudaSetDevice(opt->device) != cudaSuccess) return KC_ERR_CUDA;
-  SimParams sp;
-  params_from_options(*opt, sp);
-  a.gam = sp.gam;
-  a.rp = sp.rp;
-  a.op = sp.op;
-  a.ip = sp.ip;
-  a.fl = sp.fl;
-  return KC_OK;
-}
-
-}  // namespace
-
-extern "C" int kc_implicit_batch(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
-                                 int32_t* res, int32_t mode) {
-  BatchArgs a;
-  int st = batch_prepare(opt, a);
-  if (st) return st;
-  if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING && mode != KC_IMPLICIT_SORTED)
-    return KC_ERR_INVALID_CONFIG;
-  if (n <= 0) return KC_OK;
-  DevBuf dg, dd, dp, dr;
-  if (cudaMalloc(&dg.p, n * 23 * 8) || cudaMalloc(&dd.p, n * 8) || cudaMalloc(&dp.p, n * NV * 8) ||
-      cudaMalloc(&dr.p, n * 6 * 4))
-    return KC_ERR_OOM;
-  cudaMemcpy(dg.p, geom23, n * 23 * 8, cudaMemcpyHostToDevice);
-  cudaMemcpy(dd.p, dt, n * 8, cudaMemcpyHostToDevice);
-  cudaMemcpy(dp.p, pp, n * NV * 8, cudaMemcpyHostToDevice);
-  if ((st = launch_batch(n, (const double*)dg.p, (const double*)dd.p, (double*)dp.p, (int*)dr.p, a, mode, 0)))
-    return st;
-  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
-  cudaMemcpy(pp, dp.p, n * NV * 8, cudaMemcpyDeviceToHost);
-  cudaMemcpy(res, dr.p, n * 6 * 4, cudaMemcpyDeviceToHost);
-  return KC_OK;
-}
-
-extern "C" int kc_implicit_batch_device(const kc_options* opt, int64_t n, const double* geom23, const double* dt,
-                                        double* pp, int32_t* res, int32_t mode, void* stream) {
-  BatchArgs a;
-  int st = batch_prepare(opt, a);
-  if (st) return st;
-  if (n <= 0) return KC_OK;
-  if (!geom23 || !dt || !pp || !res) return KC_ERR_INVALID_CONFIG;
-  return launch_batch(n, geom23, dt, pp, res, a, mode, (cudaStream_t)stream);
-}
-
-namespace {
-// xorshift64* (the generator family of the reference's implicit battery)
-struct XorShift {
-  uint64_t s;
-  double next() {
-    s ^= s >> 12;
-    s ^= s << 25;
-    s ^= s >> 27;
-    return (double)((s * 0x2545F4914F6CDD1DULL) >> 11) * 0x1.0p-53;
-  }
-  double pm() { return 2.0 * next() - 1.0; }
-  double loguni(double lo, double hi) { return kmath::exp(kmath::log(lo) + (kmath::log(hi) - kmath::log(lo)) * next()); }
-};
-// a spatial 3-velocity (VELR) of Lorentz factor gamma relative to the normal
-// observer, in a random direction
-void velr_with_gamma(XorShift& rng, const Geom& g, double gamma, double v[3]) {
-  double nn[3] = {rng.pm(), rng.pm(), rng.pm()};
-  double q = 0.0;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) q += nn[i] * nn[j] * g.gg[i + 1][j + 1];
-  double sc = kmath::sqrt((gamma * gamma - 1.0) / q);
-  for (int i = 0; i < 3; ++i) v[i] = nn[i] * sc;
-}
-}  // namespace
-
-extern "C" int kc_synth_implicit_cells(const kc_options* opt, int64_t n, uint64_t seed, double* geom23, double* dt,
-                                       double* pp) {
-  if (!opt || opt->abi_version != KC_ABI_VERSION || n < 0 || !geom23 || !dt || !pp) return KC_ERR_INVALID_CONFIG;
-  SimParams sp;
-  params_from_options(*opt, sp);
-  const Consts& con = sp.op.c;
-  const long nchunk = 4096;
-  host_par(0, (n + nchunk - 1) / nchunk, [&](long k) {
-    XorShift rng{seed ^ (0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1))};
-    for (long c = k * nchunk; c < n && c < (k + 1) * nchunk; ++c) {
-      double r = rng.loguni(3.0, 50.0);
-      double th = 0.3 + (KP_PI - 0.6) * rng.next();
-      double x[4] = {0.0, kmath::log(r - sp.mp.mksr0), mks2_x2_from_theta(th, sp.mp.mksh0), 0.0};
-      Geom g;
-      geometry_at(MKS2, sp.mp, x, g);
-      double* gr = geom23 + c * 23;
-      int q = 0;
-      for (int i = 0; i < 4; ++i)
-        for (int j = i; j < 4; ++j) {
-          gr[q] = g.gg[i][j];
-          gr[10 + q] = g.GG[i][j];
-          ++q;
-        }
-      gr[20] = g.gdet;
-      gr[21] = g.alpha;
-      gr[22] = g.gttpert;
-      double* p = pp + c * NV;
-      double rho = rng.loguni(1.0e-8, 1.0);
-      double tgas = rng.loguni(1.0e5, 1.0e9);
-      double ugas = u_from_trho(con, tgas, rho, sp.gam);
-      double v[3];
-      velr_with_gamma(rng, g, 1.0 / kmath::sqrt(1.0 - 0.81 * rng.next()), v);  // |v| < 0.9c
-      p[RHO] = rho;
-      p[UU] = ugas;
-      p[VX] = v[0];
-      p[VY] = v[1];
-      p[VZ] = v[2];
-      p[ENTR] = s_from_u(rho, ugas, sp.gam);
-      double beta = rng.loguni(1.0, 1.0e3);
-      double bsq = 2.0 * (sp.gam - 1.0) * ugas / beta;
-      velr_with_gamma(rng, g, kmath::sqrt(1.0 + bsq), v);
-      p[B1] = v[0];
-      p[B2] = v[1];
-      p[B3] = v[2];
-      p[EE] = ugas / rng.loguni(1.0e-4, 1.0e4);  // E_gas / E_rad log-uniform in [1e-4, 1e4]
-      velr_with_gamma(rng, g, 1.0 + rng.next(), v);
-      p[FX] = v[0];
-      p[FY] = v[1];
-      p[FZ] = v[2];
-      dt[c] = rng.loguni(1.0e-10, 1.0);
-    }
-  });
-  return KC_OK;
-}
-
-extern "C" int kc_u2p_batch(const kc_options* opt, int64_t n, const double* geom23, const double* uu, double* pp,
-                            int32_t* flags_out) {
-  BatchArgs a;
-  int st = batch_prepare(opt, a);
-  if (st) return st;
-  if (n <= 0) return KC_OK;
-  DevBuf dg, du, dp, df;
-  if (cudaMalloc(&dg.p, n * 23 * 8) || cudaMalloc(&du.p, n * NV * 8) || cudaMalloc(&dp.p, n * NV * 8) ||
-      cudaMalloc(&df.p, n * 3 * 4))
-    return KC_ERR_OOM;
-  cudaMemcpy(dg.p, geom23, n * 23 * 8, cudaMemcpyHostToDevice);
-  cudaMemcpy(du.p, uu, n * NV * 8, cudaMemcpyHostToDevice);
-  cudaMemcpy(dp.p, pp, n * NV * 8, cudaMemcpyHostToDevice);
-  k_u2p_batch<<<nblk(n), TPB>>>(n, (const double*)dg.p, (const double*)du.p, (double*)dp.p, (int*)df.p, a);
-  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
-  cudaMemcpy(pp, dp.p, n * NV * 8, cudaMemcpyDeviceToHost);
-  cudaMemcpy(flags_out, df.p, n * 3 * 4, cudaMemcpyDeviceToHost);
-  return KC_OK;
-}
-
-// ==== allocation-free implicit batch ==========================================
-// kc_implicit_batch stages the caller's host arrays through device buffers it
-// allocates per call. This variant stages them through one fixed, file-scope
-// device array instead and allocates nothing: 16384 cells of geometry (23 f64),
-// dt (1 f64), primitives (13 f64) and results (6 i32), 5 MiB, held by every
-// device that loads the library until the process exits. The address of the
-// array on a device is looked up once, with that device current, on the first
-// call on that device (that first call should come before any stream capture).
-// All calls on a device share the array and leave the last call's contents in
-// it; calls that overlap on the same device race on it.
-namespace {
-
-const size_t kNoAllocGeomOff = 0;
-const size_t kNoAllocDtOff = kNoAllocGeomOff + (size_t)KC_NOALLOC_MAX_CELLS * 23 * 8;
-const size_t kNoAllocPpOff = kNoAllocDtOff + (size_t)KC_NOALLOC_MAX_CELLS * 8;
-const size_t kNoAllocResOff = kNoAllocPpOff + (size_t)KC_NOALLOC_MAX_CELLS * NV * 8;
-const size_t kNoAllocBytes = kNoAllocResOff + (size_t)KC_NOALLOC_MAX_CELLS * 6 * 4;
-static_assert(kNoAllocDtOff % 256 == 0 && kNoAllocPpOff % 256 == 0 && kNoAllocResOff % 256 == 0,
-              "scratch regions stay 256-byte aligned");
-
-// host-side stand-in for the device array; its device address comes from
-// cudaGetSymbolAddress
-static __device__ __align__(256) unsigned char kc_noalloc_scratch[kNoAllocBytes];
-
-const int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// the scratch array's address on the current device (set-up on first use)
-int noalloc_scratch(unsigned char** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return KC_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, kc_noalloc_scratch) != cudaSuccess || !ptr) return KC_ERR_CUDA;
-    g_noalloc_ptr[dev] = (unsigned char*)ptr;
-  }
-  *out = g_noalloc_ptr[dev];
-  return KC_OK;
-}
-
-}  // namespace
-
-extern "C" int kc_implicit_batch_noalloc(const kc_options* opt, int64_t n, const double* geom23, const double* dt,
-                                         double* pp, int32_t* res, int32_t mode) {
-  if (n > KC_NOALLOC_MAX_CELLS) return KC_ERR_TOO_MANY_CELLS;
-  BatchArgs a;
-  int st = batch_prepare(opt, a);
-  if (st) return st;
-  if (mode != KC_IMPLICIT_PER_CELL) return KC_ERR_INVALID_CONFIG;
-  if (n <= 0) return KC_OK;
-  if (!geom23 || !dt || !pp || !res) return KC_ERR_INVALID_CONFIG;
-  unsigned char* base = nullptr;
-  if ((st = noalloc_scratch(&base))) return st;
-  double* dg = (double*)(base + kNoAllocGeomOff);
-  double* dd = (double*)(base + kNoAllocDtOff);
-  double* dp = (double*)(base + kNoAllocPpOff);
-  int* dr = (int*)(base + kNoAllocResOff);
-  // every result entry of the n cells is written by the kernel; cleared anyway so
-  // that nothing of an earlier call can be read back
-  if (cudaMemset(dr, 0, (size_t)n * 6 * 4) != cudaSuccess ||
-      cudaMemcpy(dg, geom23, (size_t)n * 23 * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(dd, dt, (size_t)n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(dp, pp, (size_t)n * NV * 8, cudaMemcpyHostToDevice) != cudaSuccess)
-    return KC_ERR_CUDA;
-  k_implicit_batch<<<nblk(n), TPB>>>(n, dg, dd, dp, dr, a);
-  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
-  if (cudaMemcpy(pp, dp, (size_t)n * NV * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(res, dr, (size_t)n * 6 * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
-    return KC_ERR_CUDA;
-  return KC_OK;
-}
-
-// ---- the learned-guess network: training, forward and gradient entry points --
-namespace {
-static_assert(MLP_NW == KC_MLP_NWEIGHTS, "weight blob size");
-// minibatch indices of one training step: splitmix64 of (seed, step, slot)
-__global__ void k_mlp_sample(long* idx, long nb, long n, uint64_t seed, long step) {
-  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb) return;
-  uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(step * nb + i + 1);
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-  z ^= z >> 31;
-  idx[i] = (long)(z % (uint64_t)n);
-}
-const int MLP_ACT = MLP_IN + 4 * MLP_H + MLP_OUT;  // per-sample training record (floats)
-int mlp_device() {
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return KC_ERR_NO_DEVICE;
-  return KC_OK;
-}
-}  // namespace
-
-extern "C" int kc_mlp_forward(const float* weights, int64_t n, const float* features_std, float* out_std) {
-  int st = mlp_device();
-  if (st) return st;
-  if (!weights || n < 0 || (n > 0 && (!features_std || !out_std))) return KC_ERR_INVALID_CONFIG;
-  if (n == 0) return KC_OK;
-  DevBuf db, dw1, dw2, dw3, dx, dy;
-  if (cudaMalloc(&db.p, MLP_NW * 4) || cudaMalloc(&dw1.p, MLP_H * MLP_IN * 2) || cudaMalloc(&dw2.p, MLP_H * MLP_H * 2) ||
-      cudaMalloc(&dw3.p, 8 * MLP_H * 2) || cudaMalloc(&dx.p, n * MLP_IN * 4) || cudaMalloc(&dy.p, n * MLP_OUT * 4))
-    return KC_ERR_OOM;
-  cudaMemcpy(db.p, weights, MLP_NW * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(dx.p, features_std, n * MLP_IN * 4, cudaMemcpyHostToDevice);
-  k_mlp_pack<<<(MLP_H * MLP_H + 127) / 128, 128>>>((const float*)db.p, (__nv_bfloat16*)dw1.p, (__nv_bfloat16*)dw2.p,
-                                                   (__nv_bfloat16*)dw3.p);
-  MlpDev m = {(const __nv_bfloat16*)dw1.p, (const __nv_bfloat16*)dw2.p, (const __nv_bfloat16*)dw3.p,
-              (const float*)db.p};
-  k_mlp_forward<<<nblk(n), TPB>>>(m, n, (const float*)dx.p, (float*)dy.p);
-  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
-  cudaMemcpy(out_std, dy.p, n * MLP_OUT * 4, cudaMemcpyDeviceToHost);
-  return KC_OK;
-}
-
-extern "C" int kc_mlp_grad(const float* weights, int64_t n, const float* features_std, const float* targets_std,
-                           float* grad, float* loss) {
-  int st = mlp_device();
-  if (st) return st;
-  if (!weights || !grad || !loss || n <= 0 || !features_std || !targets_std) return KC_ERR_INVALID_CONFIG;
-  DevBuf db, dx, dt, da, dg, dl;
-  if (cudaMalloc(&db.p, MLP_NW * 4) || cudaMalloc(&dx.p, n * MLP_IN * 4) || cudaMalloc(&dt.p, n * MLP_OUT * 4) ||
-      cudaMalloc(&da.p, n * MLP_ACT * 4) || cudaMalloc(&dg.p, MLP_NW * 4) || cudaMalloc(&dl.p, 4))
-    return KC_ERR_OOM;
-  cudaMemcpy(db.p, weights, MLP_NW * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(dx.p, features_std, n * MLP_IN * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(dt.p, targets_std, n * MLP_OUT * 4, cudaMemcpyHostToDevice);
-  cudaMemset(dg.p, 0, MLP_NW * 4);
-  cudaMemset(dl.p, 0, 4);
-  k_mlp_train_fwd<<<nblk(n), TPB>>>((const float*)db.p, (const float*)dx.p, (const float*)dt.p, nullptr, n,
-                                    (float*)da.p, (float*)dl.p);
-  k_mlp_train_grad<<<(MLP_NW + 127) / 128, 128>>>((const float*)da.p, n, (float*)dg.p);
-  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
-  cudaMemcpy(grad, dg.p, MLP_NW * 4, cudaMemcpyDeviceToHost);
-  float l = 0.0f;
-  cudaMemcpy(&l, dl.p, 4, cudaMemcpyDeviceToHost);
-  *loss = l / (float)(n * MLP_OUT);
-  return KC_OK;
-}
-
-// Training: the normalisation (per-column mean and standard deviation) is
-// taken from the pairs on the host, the feature deviations floored at
-// MLP_FEATURE_STD_MIN and the standardised features clipped to
-// +-MLP_STD_CLIP as inference clips them; the weights start He-uniform
-// from `seed` (biases zero); each step draws `batch` pairs, runs the forward
-// and backward kernels and an Adam update with learning rate `lr`.
-extern "C" int kc_mlp_train(const float* features, const float* targets, int64_t n, int32_t steps, int32_t batch,
-                            float lr, uint64_t seed, float* weights_out, float* loss_curve) {
-  int st = mlp_device();
-  if (st) return st;
-  if (!features || !targets || !weights_out || n <= 0 || steps < 0 || batch <= 0 || !(lr > 0.0f))
-    return KC_ERR_INVALID_CONFIG;
-  std::vector<float> w(MLP_NW, 0.0f), xs((size_t)n * MLP_IN), ts((size_t)n * MLP_OUT);
-  auto standardise = [&](const float* src, int cols, int off_mean, int off_std, double floor, double clip,
-                         float* dst) {
-    for (int k = 0; k < cols; ++k) {
-      double s = 0.0, q = 0.0;
-      for (int64_t i = 0; i < n; ++i) s += src[i * cols + k];
-      double mu = s / (double)n;
-      for (int64_t i = 0; i < n; ++i) q += (src[i * cols + k] - mu) * (src[i * cols + k] - mu);
-      double sd = std::sqrt(q / (double)n);
-      if (!(sd > floor)) sd = floor;
-      w[off_mean + k] = (float)mu;
-      w[off_std + k] = (float)sd;
-      for (int64_t i = 0; i < n; ++i) {
-        double z = ((double)src[i * cols + k] - (double)w[off_mean + k]) / (double)w[off_std + k];
-        dst[i * cols + k] = (float)(z > clip ? clip : (z < -clip ? -clip : z));
-      }
-    }
-  };
-  standardise(features, MLP_IN, MLP_OFF_IMEAN, MLP_OFF_ISTD, MLP_FEATURE_STD_MIN, MLP_STD_CLIP, xs.data());
-  standardise(targets, MLP_OUT, MLP_OFF_OMEAN, MLP_OFF_OSTD, 1.0e-30, 1.0e30, ts.data());
-  for (float v : xs)
-    if (!std::isfinite(v)) return KC_ERR_INVALID_CONFIG;
-  for (float v : ts)
-    if (!std::isfinite(v)) return KC_ERR_INVALID_CONFIG;
-  XorShift rng{seed ? seed : 0x2545F4914F6CDD1DULL};
-  auto he = [&](int off, int rows, int cols) {
-    double a = std::sqrt(6.0 / cols);
-    for (int i = 0; i < rows * cols; ++i) w[off + i] = (float)(a * rng.pm());
-  };
-  he(MLP_OFF_W1, MLP_H, MLP_IN);
-  he(MLP_OFF_W2, MLP_H, MLP_H);
-  he(MLP_OFF_W3, MLP_OUT, MLP_H);
-  long nb = batch < n ? batch : n;
-  DevBuf db, dg, dm1, dm2, dx, dt, di, da, dl;
-  if (cudaMalloc(&db.p, MLP_NW * 4) || cudaMalloc(&dg.p, MLP_NW * 4) || cudaMalloc(&dm1.p, MLP_NW * 4) ||
-      cudaMalloc(&dm2.p, MLP_NW * 4) || cudaMalloc(&dx.p, n * MLP_IN * 4) || cudaMalloc(&dt.p, n * MLP_OUT * 4) ||
-      cudaMalloc(&di.p, nb * 8) || cudaMalloc(&da.p, nb * MLP_ACT * 4) || cudaMalloc(&dl.p, (steps + 1) * 4))
-    return KC_ERR_OOM;
-  cudaMemcpy(db.p, w.data(), MLP_NW * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(dx.p, xs.data(), n * MLP_IN * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(dt.p, ts.data(), n * MLP_OUT * 4, cudaMemcpyHostToDevice);
-  cudaMemset(dm1.p, 0, MLP_NW * 4);
-  cudaMemset(dm2.p, 0, MLP_NW * 4);
-  cudaMemset(dl.p, 0, (steps + 1) * 4);
-  double b1 = 1.0, b2 = 1.0;
-  for (int s = 0; s < steps; ++s) {
-    b1 *= 0.9;
-    b2 *= 0.999;
-    k_mlp_sample<<<nblk(nb), TPB>>>((long*)di.p, nb, n, seed, s);
-    k_mlp_train_fwd<<<nblk(nb), TPB>>>((const float*)db.p, (const float*)dx.p, (const float*)dt.p,
-                                       (const long*)di.p, nb, (float*)da.p, (float*)dl.p + s);
-    k_mlp_train_grad<<<(MLP_NW + 127) / 128, 128>>>((const float*)da.p, nb, (float*)dg.p);
-    k_mlp_adam<<<(MLP_NW + 127) / 128, 128>>>((float*)db.p, (const float*)dg.p, (float*)dm1.p, (float*)dm2.p, lr,
-                                              (float)(1.0 - b1), (float)(1.0 - b2));
-  }
-  if (cudaDeviceSynchronize() != cudaSuccess) return KC_ERR_CUDA;
-  cudaMemcpy(weights_out, db.p, MLP_NW * 4, cudaMemcpyDeviceToHost);
-  if (loss_curve && steps > 0) {
-    std::vector<float> l(steps);
-    cudaMemcpy(l.data(), dl.p, steps * 4, cudaMemcpyDeviceToHost);
-    for (int s = 0; s < steps; ++s) loss_curve[s] = l[s] / (float)(nb * MLP_OUT);
-  }
-  return KC_OK;
-}
-
-// ---- FP64 pipe peak: a DFMA-chain microbenchmark (the FP64 roofline) -------------
-namespace {
-const int DFMA_CHAINS = 16;
-__global__ void __launch_bounds__(256) k_dfma_chains(double* sink, int iters, double b, double c) {
-  double a[DFMA_CHAINS];
-  for (int k = 0; k < DFMA_CHAINS; ++k) a[k] = 1.0e-3 * (threadIdx.x + k);
-  for (int i = 0; i < iters; ++i)
-#pragma unroll
-    for (int k = 0; k < DFMA_CHAINS; ++k) a[k] = __fma_rn(a[k], b, c);
-  double s = 0.0;
-  for (int k = 0; k < DFMA_CHAINS; ++k) s += a[k];
-  if (s == -1.0) sink[blockIdx.x] = s;  // never true; keeps the chains live
-}
-}  // namespace
-
-// Best of five launches of independent DFMA chains over every SM, in TFLOP/s
-// (2 FLOP per DFMA). Runs on the current device.
-extern "C" int kc_fp64_peak(double* tflops) {
-  int st = mlp_device();
-  if (st) return st;
-  if (!tflops) return KC_ERR_INVALID_CONFIG;
-  int dev = 0, nsm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int blocks = nsm * 8, threads = 256, iters = 1 << 14;
-  DevBuf sink;
-  if (cudaMalloc(&sink.p, (size_t)blocks * 8)) return KC_ERR_OOM;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  k_dfma_chains<<<blocks, threads>>>((double*)sink.p, 256, 0.999999, 1.0e-7);
-  float best = 1.0e30f;
-  for (int r = 0; r < 5; ++r) {
-    cudaEventRecord(e0);
-    k_dfma_chains<<<blocks, threads>>>((double*)sink.p, iters, 0.999999, 1.0e-7);
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) best = ms;
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (cudaGetLastError() != cudaSuccess) return KC_ERR_CUDA;
-  *tflops = 2.0 * DFMA_CHAINS * (double)iters * blocks * threads / (best * 1.0e-3) / 1.0e12;
-  return KC_OK;
-}
-
-// ---- autotuner -------------------------------------------------------------------
-namespace {
-struct TuneConfig {
-  int implicit_mode, tpb_implicit, tpb_flux, tpb_u2p, phi_fastest;
-};
-void tune_apply(kc_handle* h, const TuneConfig& c) {
-  h->opt.implicit_mode = c.implicit_mode;
-  h->implicit_phi_fastest = c.phi_fastest;
-  h->tpb_implicit = c.tpb_implicit;
-  h->tpb_flux = c.tpb_flux;
-  h->tpb_u2p = c.tpb_u2p;
-  drop_graph(h);
-}
-TuneConfig tune_current(const kc_handle* h) {
-  return {h->opt.implicit_mode, h->tpb_implicit, h->tpb_flux, h->tpb_u2p, h->implicit_phi_fastest};
-}
-// The state a step reads and writes across steps: p, u, flags on the device and
-// the handle's step scalars and counters.
-struct TuneSnapshot {
-  double *p = nullptr, *u = nullptr;
-  int* flags = nullptr;
-  kc_counters c;
-  long long n_launch = 0;
-};
-void tune_save(kc_handle* h, TuneSnapshot& sn) {
-  size_t nb = (size_t)NV * h->gr.nc * 8;
-  cudaMemcpyAsync(sn.p, h->ds.p, nb, cudaMemcpyDeviceToDevice, h->stream);
-  cudaMemcpyAsync(sn.u, h->ds.u, nb, cudaMemcpyDeviceToDevice, h->stream);
-  cudaMemcpyAsync(sn.flags, h->ds.flags, (size_t)6 * h->gr.nc * 4, cudaMemcpyDeviceToDevice, h->stream);
-  kc_get_counters(h, &sn.c);
-  sn.n_launch = h->n_launch;
-}
-void tune_restore(kc_handle* h, const TuneSnapshot& sn) {
-  size_t nb = (size_t)NV * h->gr.nc * 8;
-  cudaMemcpyAsync(h->ds.p, sn.p, nb, cudaMemcpyDeviceToDevice, h->stream);
-  cudaMemcpyAsync(h->ds.u, sn.u, nb, cudaMemcpyDeviceToDevice, h->stream);
-  cudaMemcpyAsync(h->ds.flags, sn.flags, (size_t)6 * h->gr.nc * 4, cudaMemcpyDeviceToDevice, h->stream);
-  kc_set_counters(h, &sn.c);
-  h->n_launch = sn.n_launch;
-}
-}  // namespace
-
-// Picks the implicit form (per-cell or split), the block sizes of the
-// per-cell implicit, face-flux and u2p kernels and the per-cell implicit
-// kernel's cell order (phi on 3D or theta on 2D fastest, or x fastest) by
-// timing whole steps on the
-// handle's current state, one knob at a time (coordinate descent from the
-// configuration on entry). Each trial restores the state, runs one untimed step
-// (with the graph form on, a second one, so the timed steps replay the graph)
-// and times `steps` steps with CUDA events on the handle's stream. Every
-// candidate gives bit-identical results, so the choice changes speed only. The
-// state and counters are restored at the end, and the best configuration stays
-// set. The learned guess and the harvest keep their fixed forms (not tuned
-// while either is on).
-extern "C" int kc_autotune(kc_handle* h, int32_t steps, kc_tune_result* out) {
-  if (!h || steps < 1) return KC_ERR_INVALID_CONFIG;
-  if (h->last_status) return h->last_status;
-  if (h->guess_mode != KC_GUESS_PLAIN || h->hcap > 0)
-    return reject(h, KC_ERR_INVALID_CONFIG, "autotune with the learned guess or the harvest on");
-  if (h->timing) return reject(h, KC_ERR_INVALID_CONFIG, "autotune with pass timing on");
-  int st = cuda_check(h, cudaStreamSynchronize(h->stream), "autotune");
-  if (st) return st;
-  TuneSnapshot sn;
-  size_t nb = (size_t)NV * h->gr.nc * 8;
-  if (cudaMalloc(&sn.p, nb) || cudaMalloc(&sn.u, nb) || cudaMalloc(&sn.flags, (size_t)6 * h->gr.nc * 4)) {
-    cudaFree(sn.p);
-    cudaFree(sn.u);
-    cudaFree(sn.flags);
-    return fail(h, KC_ERR_OOM, "autotune snapshot");
-  }
-  tune_save(h, sn);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  int trials = 0;
-  auto measure = [&](const TuneConfig& c, double& ms) -> int {
-    tune_restore(h, sn);
-    tune_apply(h, c);
-    int warm = h->use_graph ? 2 : 1;
-    for (int k = 0; k < warm; ++k)
-      if (int r = run_step(h, NAN, nullptr)) return r;
-    cudaEventRecord(e0, h->stream);
-    for (int k = 0; k < steps; ++k)
-      if (int r = run_step(h, NAN, nullptr)) return r;
-    cudaEventRecord(e1, h->stream);
-    cudaEventSynchronize(e1);
-    float f = 0.0f;
-    cudaEventElapsedTime(&f, e0, e1);
-    ms = f / steps;
-    ++trials;
-    return KC_OK;
-  };
-  TuneConfig best = tune_current(h), entry = best;
-  double best_ms = 0.0, entry_ms = 0.0;
-  st = measure(best, best_ms);
-  entry_ms = best_ms;
-  const int forms[2] = {KC_IMPLICIT_PER_CELL, KC_IMPLICIT_SPLIT};
-  const int sizes[3] = {64, 96, 128};
-  for (int knob = 0; knob < 5 && !st; ++knob) {
-    int n = (knob == 0 || knob == 4) ? 2 : 3;
-    for (int i = 0; i < n && !st; ++i) {
-      TuneConfig c = best;
-      if (knob == 0) c.implicit_mode = forms[i];
-      if (knob == 1) c.tpb_implicit = sizes[i];
-      if (knob == 2) c.tpb_flux = sizes[i];
-      if (knob == 3) c.tpb_u2p = sizes[i];
-      if (knob == 4) c.phi_fastest = i;
-      if (memcmp(&c, &best, sizeof c) == 0) continue;
-      double ms = 0.0;
-      st = measure(c, ms);
-      if (!st && ms < best_ms) {
-        best_ms = ms;
-        best = c;
-      }
-    }
-  }
-  tune_restore(h, sn);
-  tune_apply(h, st ? entry : best);
-  cudaStreamSynchronize(h->stream);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaFree(sn.p);
-  cudaFree(sn.u);
-  cudaFree(sn.flags);
-  if (st) return st;
-  if (out) {
-    out->implicit_mode = best.implicit_mode;
-    out->tpb_implicit = best.tpb_implicit;
-    out->tpb_flux = best.tpb_flux;
-    out->tpb_u2p = best.tpb_u2p;
-    out->implicit_phi_fastest = best.phi_fastest;
-    out->ms_per_step = best_ms;
-    out->ms_per_step_entry = entry_ms;
-    out->trials = trials;
-  }
-  return KC_OK;
-}
-
-// ---- KDMP v2 checkpoints (koral/io/dump.zig) ---------------------------------------
-extern "C" int kc_kdmp_write_header(const kc_dump_header* hd, uint8_t* out) {
-  if (!hd || !out) return KC_ERR_INVALID_CONFIG;
-  kdump::write_header(*hd, out);
-  return KC_OK;
-}
-extern "C" int kc_kdmp_parse_header(const uint8_t* bytes, int64_t len, kc_dump_header* hd) {
-  if (!hd) return KC_ERR_INVALID_CONFIG;
-  return kdump::parse_header(bytes, len, *hd);
-}
-extern "C" int64_t kc_kdmp_size(kc_handle* h) {
-  if (!h) return -1;
-  return KC_KDMP_HEADER_SIZE + kdump::body_bytes(h->gr.nx, h->gr.ny, h->gr.nz, NV);
-}
-extern "C" int kc_kdmp_write(kc_handle* h, uint32_t out_idx, uint8_t* out, int64_t capacity, int64_t* written) {
-  if (!h || !out) return KC_ERR_INVALID_CONFIG;
-  if (written) *written = 0;
-  int64_t need = kc_kdmp_size(h);
-  if (capacity < need) return reject(h, KC_ERR_INVALID_CONFIG, "KDMP buffer smaller than kc_kdmp_size");
-  const DGrid& gr = h->gr;
-  long nd = (long)gr.nx * gr.ny * gr.nz;
-  // the staging array holds NV x (cells incl. ghosts) doubles, more than the body
-  k_domain_to_kdmp<<<nblk(nd * NV, 256), 256, 0, h->stream>>>(h->ds, h->staging);
-  int st = cuda_check(h, cudaMemcpyAsync(out + KC_KDMP_HEADER_SIZE, h->staging, (size_t)nd * NV * 8,
-                                         cudaMemcpyDeviceToHost, h->stream), "KDMP write");
-  if (!st) st = cuda_check(h, cudaStreamSynchronize(h->stream), "KDMP write");
-  if (st) return st;
-  kc_dump_header hd = {(uint32_t)gr.nx, (uint32_t)gr.ny, (uint32_t)gr.nz, (uint32_t)NV, h->t, (uint64_t)h->nstep,
-                       out_idx};
-  kdump::write_header(hd, out);
-  if (written) *written = need;
-  return KC_OK;
-}
-extern "C" int kc_kdmp_load(kc_handle* h, const uint8_t* bytes, int64_t len, kc_dump_header* hd_out) {
-  if (!h) return KC_ERR_INVALID_CONFIG;
-  kc_dump_header hd;
-  int st = kdump::parse_header(bytes, len, hd);
-  if (st) return reject(h, st, "KDMP header");
-  const DGrid& gr = h->gr;
-  if (hd.nx != (uint32_t)gr.nx || hd.ny != (uint32_t)gr.ny || hd.nz != (uint32_t)gr.nz || hd.nv != (uint32_t)NV)
-    return reject(h, KC_ERR_KDMP_DIM_MISMATCH, "KDMP grid differs from the handle's");
-  long nd = (long)gr.nx * gr.ny * gr.nz;
-  if (len < kc_kdmp_size(h)) return reject(h, KC_ERR_KDMP_TRUNCATED, "KDMP body truncated");
-  st = cuda_check(h, cudaMemcpyAsync(h->staging, bytes + KC_KDMP_HEADER_SIZE, (size_t)nd * NV * 8,
-                                     cudaMemcpyHostToDevice, h->stream), "KDMP load");
-  if (st) return st;
-  k_kdmp_to_domain<<<nblk(nd), TPB, 0, h->stream>>>(h->ds, h->staging, h->sp.gam);
-  st = cuda_check(h, cudaStreamSynchronize(h->stream), "KDMP load");
-  if (st) return st;
-  if (hd_out) *hd_out = hd;
-  return KC_OK;
-}
-extern "C" int kc_kdmp_write_file(kc_handle* h, const char* path, uint32_t out_idx) {
-  if (!h || !path) return KC_ERR_INVALID_CONFIG;
-  int64_t n = kc_kdmp_size(h);
-  std::vector<uint8_t> buf((size_t)n);
-  int st = kc_kdmp_write(h, out_idx, buf.data(), n, nullptr);
-  if (st) return st;
-  FILE* f = fopen(path, "wb");
-  if (!f) return reject(h, KC_ERR_IO, std::string("cannot create ") + path);
-  size_t w = fwrite(buf.data(), 1, buf.size(), f);
-  int c = fclose(f);
-  if (w != buf.size() || c != 0) return reject(h, KC_ERR_IO, std::string("cannot write ") + path);
-  return KC_OK;
-}
-extern "C" int kc_kdmp_load_file(kc_handle* h, const char* path, kc_dump_header* hd) {
-  if (!h || !path) return KC_ERR_INVALID_CONFIG;
-  FILE* f = fopen(path, "rb");
-  if (!f) return reject(h, KC_ERR_IO, std::string("cannot open ") + path);
-  std::vector<uint8_t> buf;
-  uint8_t chunk[1 << 16];
-  size_t r;
-  while ((r = fread(chunk, 1, sizeof chunk, f)) > 0) buf.insert(buf.end(), chunk, chunk + r);
-  bool err = ferror(f) != 0;
-  fclose(f);
-  if (err) return reject(h, KC_ERR_IO, std::string("cannot read ") + path);
-  return kc_kdmp_load(h, buf.data(), (int64_t)buf.size(), hd);
-}
+#include "kc_abi_batch.inc"
+#include "kc_abi_mlp.inc"
+#include "kc_abi_fp64_peak.inc"
+#include "kc_abi_autotune.inc"
+#include "kc_abi_kdmp.inc"

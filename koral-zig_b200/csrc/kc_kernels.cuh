@@ -367,7 +367,7 @@ __device__ int puffy_bc_cell(const DevState& s, long ix, long iy, long iz, int f
   const long nx = s.gr.nx, ny = s.gr.ny, nc = s.gr.nc;
   if (face == 1) {
     load_cell(s.p, nc, cidx(s.gr, nx - 1, iy, iz), pp);
-    Geom geo, gbl, gbd;
+    Geom geo, gbl;
     geom_cell(s, ix, iy, iz, geo);
     long c = cidx(s.gr, ix, iy, iz);
     geom_bl(s, c, gbl);

@@ -221,12 +221,11 @@ def test_implicit_rung_ladder():
     z = run_golden("rad_implicit", i, 19)
     st = _implicit_stats(i, o, z)
     print("implicit golden:", st)
-    # The reference gates ok-agreement at 97% (Zig vs C; 97.6% observed there).
-    # This restatement uses its own transcendental library; on these records it
-    # reaches 306/316 = 96.8%, and 97.2% with glibc's correctly rounded pow in
-    # place of the Go/Zig repeated-squaring pow: the flips are stiff records at
-    # the edge of convergence, decided by last-bit rounding. Gate at 96%.
-    assert st["ok_agree"] * 100 >= st["basis"] * 96, st
+    # The reference's gate (koral/tests/golden/implicit_golden_tests.zig:50-168):
+    # ok-agreement with C KORAL >= 97% (307/315 here). The flips are stiff
+    # records at the edge of convergence, decided by last-bit rounding of C's
+    # glibc transcendentals against the fdlibm ones the Zig path uses.
+    assert st["ok_agree"] * 100 >= st["basis"] * 97, st
     assert st["entropy_flip"] <= 30, st
     assert st["rung_agree"] * 10 >= st["both_ok"] * 9, st
     assert st["compared"] >= 40, st

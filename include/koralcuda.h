@@ -3,7 +3,7 @@
  * The reference (koral-zig) has no FFI: its step path sits behind the Zig
  * generic `Sim(cfg)` (koral/sim.zig:93). Each entry point below replaces one
  * method or field of that type, cited as file:line in koral-zig; a Zig host
- * binds them with `extern fn` (see INTEGRATION.md). All structs are POD,
+ * binds them with `extern fn`. All structs are POD,
  * all arrays are caller-owned host memory copied at the call, and no call
  * aborts: every failure is an int status plus kc_last_error().
  *
@@ -230,7 +230,14 @@ int kc_get_launch_count(kc_handle* h, int64_t* n);
 
 /* Engine forms (no reference counterpart) */
 int kc_set_precision(kc_handle* h, int32_t mode);
+/* Selecting KC_IMPLICIT_SPLIT allocates that form's compact list; when that
+ * fails the call returns KC_ERR_OOM and the form stays as it was. */
 int kc_set_implicit_mode(kc_handle* h, int32_t mode);
+/* Test hook (no reference counterpart): the n-th next optional allocation (of
+ * the split form's list, the learned guess's buffers, the harvest records and
+ * their counters) fails as if the device were full, so the call that makes it
+ * returns KC_ERR_OOM with nothing half-allocated kept; 0 disarms. */
+int kc_debug_fail_allocs(kc_handle* h, int32_t n);
 /* The step as a CUDA graph: with on != 0 the whole step's launch sequence
  * (every pass of koral/sim.zig:1792 step, and the copy of its dt-derived
  * coefficients from a pinned table) is captured once and replayed each step;
@@ -369,9 +376,12 @@ int kc_synth_implicit_cells(const kc_options* opt, int64_t n, uint64_t seed, dou
  * allocator holding the device) or a fixed-budget process. The arrays are
  * staged through one fixed device array of KC_NOALLOC_MAX_CELLS cells (5 MiB),
  * held by every device that loads the library until exit; n above the maximum
- * returns KC_ERR_TOO_MANY_CELLS. The first call on a device looks up that
- * array's address with the device current (make that first call before any
- * stream capture). Calls share the array: calls that overlap on one device race. */
+ * returns KC_ERR_TOO_MANY_CELLS. Only mode KC_IMPLICIT_PER_CELL is accepted
+ * (others return KC_ERR_INVALID_CONFIG: those forms need stream-ordered
+ * scratch). The first call on a device looks up that array's address with the
+ * device current. Every call is synchronous (blocking copies and a device
+ * synchronize), so none may be made while a stream capture is active on the
+ * device. Calls share the array: calls that overlap on one device race. */
 #define KC_NOALLOC_MAX_CELLS 16384
 int kc_implicit_batch_noalloc(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
                               int32_t* res, int32_t mode);

@@ -121,6 +121,7 @@ struct kc_handle {
   long long nstep = 0, n_fail = 0, n_fail_step = 0, n_iters = 0, n_solves = 0, n_guard = 0;
   std::string err;
   int last_status = 0;
+  int fail_alloc_at = 0;  // host-side test hook: the n-th next optional allocation fails (0: none)
 };
 
 namespace {
@@ -156,6 +157,36 @@ T* dalloc(kc_handle* h, size_t n, int& st) {
   cudaMemset(p, 0, n * sizeof(T) + 16);
   h->allocs.push_back(p);
   return (T*)p;
+}
+// An allocation for an optional form (the split implicit buffers, the learned
+// guess, the harvest records): on failure nothing is published, the message
+// is kept for kc_last_error, the handle stays usable and nullptr is returned.
+template <class T>
+T* try_dalloc(kc_handle* h, size_t n) {
+  if (h->fail_alloc_at > 0 && --h->fail_alloc_at == 0) {
+    h->err = "cudaMalloc: out of memory (injected)";
+    return nullptr;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T) + 16);
+  if (e == cudaSuccess) e = cudaMemset(p, 0, n * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // an allocation failure is not a device fault: clear it for later checks
+    if (p) cudaFree(p);
+    h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  h->allocs.push_back(p);
+  return (T*)p;
+}
+void dfree(kc_handle* h, void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < h->allocs.size(); ++i)
+    if (h->allocs[i] == p) {
+      h->allocs.erase(h->allocs.begin() + i);
+      break;
+    }
+  cudaFree(p);
 }
 
 // ---- metric cache, built once on the device (koral/metric/precompute.zig:175) ---
@@ -328,6 +359,32 @@ void launch_do_correct(kc_handle* h) {
   k_polar_correct<<<nblk((long)gr.nx * gr.nz * 2 * ncp), TPB, 0, h->stream>>>(h->ds, h->sp.gam, ncp);
 }
 
+// The split implicit form's compact list (count, cell indices, warm starts),
+// allocated when the form is selected, outside any step and any capture; the
+// three pointers are published together or not at all.
+int ensure_split(kc_handle* h) {
+  if (h->split_count) return KC_OK;
+  const DGrid& gr = h->gr;
+  long ndom = (long)gr.nx * gr.ny * gr.nz;
+  unsigned long long* cnt = try_dalloc<unsigned long long>(h, 1);
+  int* cell = cnt ? try_dalloc<int>(h, ndom) : nullptr;
+  double* pp0 = cell ? try_dalloc<double>(h, (size_t)NV * ndom) : nullptr;
+  if (!pp0) {
+    dfree(h, cell);
+    dfree(h, cnt);
+    return reject(h, KC_ERR_OOM, h->err);
+  }
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_implicit_ladder, TPB, 0);
+  h->split_blocks = (per_sm > 0 ? per_sm : 1) * (nsm > 0 ? nsm : 1);
+  h->split_count = cnt;
+  h->split_cell = cell;
+  h->split_pp0 = pp0;
+  return KC_OK;
+}
+
 void launch_implicit(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   ImplArgs a;
@@ -342,20 +399,9 @@ void launch_implicit(kc_handle* h, int dt_slot) {
   PassScope ps(h, KC_PASS_IMPLICIT);
   // the learned guess and the harvest run in the per-cell form
   bool extra = h->guess_mode == KC_GUESS_MLP || h->hcap > 0;
-  if (h->opt.implicit_mode == KC_IMPLICIT_SPLIT && !extra) {
+  // the split form's buffers exist whenever the form is selected (ensure_split)
+  if (h->opt.implicit_mode == KC_IMPLICIT_SPLIT && !extra && h->split_count) {
     long ndom = (long)gr.nx * gr.ny * gr.nz;
-    if (!h->split_count) {
-      int st = 0;
-      h->split_count = dalloc<unsigned long long>(h, 1, st);
-      h->split_cell = dalloc<int>(h, ndom, st);
-      h->split_pp0 = dalloc<double>(h, (size_t)NV * ndom, st);
-      if (st) return;
-      int dev = 0, nsm = 0, per_sm = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_implicit_ladder, TPB, 0);
-      h->split_blocks = (per_sm > 0 ? per_sm : 1) * (nsm > 0 ? nsm : 1);
-    }
     SplitList L = {h->split_count, h->split_cell, h->split_pp0, ndom};
     cudaMemsetAsync(h->split_count, 0, sizeof(unsigned long long), h->stream);
     ++h->n_launch;
@@ -871,6 +917,7 @@ int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
   h->min_dx = mdx;
   h->min_dy = mdy;
   h->min_dz = mdz;
+  if (h->opt.implicit_mode == KC_IMPLICIT_SPLIT && (st = ensure_split(h))) return fail(h, st, h->err);
   return cuda_check(h, cudaDeviceSynchronize(), "kc_create");
 }
 
@@ -1147,6 +1194,14 @@ int kc_get_launch_count(kc_handle* h, int64_t* n) {
   return KC_OK;
 }
 
+// Test hook: the n-th next optional allocation (split-form buffers, learned
+// guess, harvest records, their counters) fails as if the device were out of
+// memory, so the OOM paths run without exhausting a shared GPU; 0 disarms.
+int kc_debug_fail_allocs(kc_handle* h, int32_t n) {
+  if (!h || n < 0) return KC_ERR_INVALID_CONFIG;
+  h->fail_alloc_at = n;
+  return KC_OK;
+}
 int kc_debug_phase(kc_handle* h, int phase, double dt) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   reset_step_scalars(h);
@@ -1200,14 +1255,17 @@ int kc_set_implicit_mode(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   if (mode != KC_IMPLICIT_PER_CELL && mode != KC_IMPLICIT_COMPACTING && mode != KC_IMPLICIT_SPLIT)
     return reject(h, KC_ERR_INVALID_CONFIG, "unknown implicit mode");
+  if (mode == KC_IMPLICIT_SPLIT) {
+    int st = ensure_split(h);
+    if (st) return st;  // the form stays as it was
+  }
   h->opt.implicit_mode = mode;
   drop_graph(h);
   return KC_OK;
 }
 static int ensure_imp_ctr(kc_handle* h) {
-  int st = 0;
-  if (!h->imp_ctr) h->imp_ctr = dalloc<unsigned long long>(h, 2, st);
-  return st;
+  if (!h->imp_ctr) h->imp_ctr = try_dalloc<unsigned long long>(h, 2);
+  return h->imp_ctr ? KC_OK : reject(h, KC_ERR_OOM, h->err);
 }
 // The CUDA graph form of the step (no reference counterpart): on, the whole
 // step's launch sequence is captured once and replayed (bit-identical).
@@ -1235,14 +1293,26 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
   int st = ensure_imp_ctr(h);
   const DGrid& gr = h->gr;
   long ndom = (long)gr.nx * gr.ny * gr.nz;
-  if (!h->mlp_blob) {
-    h->mlp_blob = dalloc<float>(h, MLP_NW, st);
-    h->mlp_w1 = dalloc<__nv_bfloat16>(h, MLP_H * MLP_IN, st);
-    h->mlp_w2 = dalloc<__nv_bfloat16>(h, MLP_H * MLP_H, st);
-    h->mlp_w3 = dalloc<__nv_bfloat16>(h, 8 * MLP_H, st);
-    h->guess = dalloc<double>(h, (size_t)NV * ndom, st);
-  }
   if (st) return st;
+  if (!h->mlp_blob) {  // the five buffers are published together or not at all
+    float* blob = try_dalloc<float>(h, MLP_NW);
+    __nv_bfloat16* w1 = blob ? try_dalloc<__nv_bfloat16>(h, MLP_H * MLP_IN) : nullptr;
+    __nv_bfloat16* w2 = w1 ? try_dalloc<__nv_bfloat16>(h, MLP_H * MLP_H) : nullptr;
+    __nv_bfloat16* w3 = w2 ? try_dalloc<__nv_bfloat16>(h, 8 * MLP_H) : nullptr;
+    double* guess = w3 ? try_dalloc<double>(h, (size_t)NV * ndom) : nullptr;
+    if (!guess) {
+      dfree(h, w3);
+      dfree(h, w2);
+      dfree(h, w1);
+      dfree(h, blob);
+      return reject(h, KC_ERR_OOM, h->err);
+    }
+    h->mlp_blob = blob;
+    h->mlp_w1 = w1;
+    h->mlp_w2 = w2;
+    h->mlp_w3 = w3;
+    h->guess = guess;
+  }
   int e = cuda_check(h, cudaMemcpyAsync(h->mlp_blob, weights, MLP_NW * 4, cudaMemcpyHostToDevice, h->stream),
                      "guess weights");
   if (e) return e;
@@ -1257,10 +1327,19 @@ int kc_harvest_implicit(kc_handle* h, int64_t capacity) {
   if (!h || capacity < 0) return KC_ERR_INVALID_CONFIG;
   int st = ensure_imp_ctr(h);
   if (st) return st;
-  if (capacity > h->hcap) {
-    h->hx = dalloc<float>(h, (size_t)capacity * MLP_IN, st);
-    h->ht = dalloc<float>(h, (size_t)capacity * MLP_OUT, st);
-    if (st) return st;
+  if (capacity > h->hcap) {  // grow: both buffers or neither; the old ones stay on failure
+    float* nx = try_dalloc<float>(h, (size_t)capacity * MLP_IN);
+    float* nt = nx ? try_dalloc<float>(h, (size_t)capacity * MLP_OUT) : nullptr;
+    if (!nt) {
+      dfree(h, nx);
+      return reject(h, KC_ERR_OOM, h->err);
+    }
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graph(h);
+    dfree(h, h->hx);
+    dfree(h, h->ht);
+    h->hx = nx;
+    h->ht = nt;
   }
   h->hcap = capacity;
   drop_graph(h);

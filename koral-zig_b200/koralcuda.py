@@ -20,6 +20,7 @@ NFLAGS = 6
 
 KC_OK = 0
 KC_ERR_INVALID_CONFIG = 1
+KC_ERR_OOM = 2
 KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
 KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT, KC_IMPLICIT_SORTED = 0, 1, 2, 3
@@ -164,6 +165,7 @@ def lib():
     L.kc_kdmp_load_file.argtypes = [vp, ctypes.c_char_p, P(KcDumpHeader)]
     L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
     L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
+    L.kc_debug_fail_allocs.argtypes = [vp, i32]
     for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
               "kc_upload_flags", "kc_download_flags", "kc_set_counters", "kc_get_counters", "kc_finish_init",
               "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p", "kc_cfl_dt", "kc_step", "kc_step_n",
@@ -173,7 +175,7 @@ def lib():
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
               "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune",
               "kc_kdmp_write_header", "kc_kdmp_parse_header", "kc_kdmp_write", "kc_kdmp_load", "kc_kdmp_write_file",
-              "kc_kdmp_load_file"]:
+              "kc_kdmp_load_file", "kc_debug_fail_allocs"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -313,6 +315,11 @@ class Sim:
         self._check(self._lib.kc_autotune(self._h, steps, ctypes.byref(r)))
         return {k: getattr(r, k) for k, _ in KcTuneResult._fields_}
 
+    def set_implicit_mode(self, mode):
+        """KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING or KC_IMPLICIT_SPLIT
+        (all bit-identical; the split form allocates its list here)."""
+        self._check(self._lib.kc_set_implicit_mode(self._h, mode))
+
     def set_precision(self, mode):
         """KC_PLAIN_FP64 or KC_MIXED (FP32 reconstruction, LAXF and flux-CT)."""
         self._check(self._lib.kc_set_precision(self._h, mode))
@@ -361,6 +368,10 @@ class Sim:
             return
         w = np.ascontiguousarray(weights, dtype=np.float32)
         self._check(self._lib.kc_set_guess(self._h, KC_GUESS_MLP, w.ctypes.data, w.size))
+
+    def debug_fail_allocs(self, n):
+        """Test hook: the n-th next optional allocation fails (KC_ERR_OOM); 0 disarms."""
+        self._check(self._lib.kc_debug_fail_allocs(self._h, int(n)))
 
     def harvest_implicit(self, capacity):
         """Collect (features, targets) of first-rung converged solves from the

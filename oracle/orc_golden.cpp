@@ -280,6 +280,24 @@ extern "C" int orc_golden(const char* name, long nrec, const double* in, int nin
       for (int i = 0; i < 4; ++i) o[i] = y[i];
       for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) o[4 + i * 4 + j] = m[i][j];
+    } else if (!strcmp(name, "frames_transpall")) {
+      // trans_pall_coco between the record's coordinate systems
+      // (koral/frames.zig:300 transPallCoco, state_golden_tests.zig:94): in =
+      // from, to, x1..x3, pp[13], geometry of `from` (20), of `to` (20)
+      auto cid = [](double v) { int id = (int)v; return id == 1 ? BL : id == 2 ? KS : id == 4 ? MINK : MKS2; };
+      MetricParams mp = {0.0, 0.1, 0.9};
+      int from = cid(a[0]), to = cid(a[1]);
+      double x[4] = {0.0, a[2], a[3], a[4]};
+      Geom g1, g2;
+      geom_from_record(a + 18, 20, g1);
+      for (int i = 0; i < 4; ++i) g1.xx[i] = x[i];
+      geom_from_record(a + 38, 20, g2);
+      double pp[NV], jac[4][4];
+      for (int i = 0; i < NV; ++i) pp[i] = a[5 + i];
+      dxdx(x, from, to, mp, jac);
+      int e = from == to ? 0 : trans_pmhd_coco_j(pp, g1, g2, jac, pp);
+      if (!e && from != to) e = trans_prad_coco_j(pp, g1, g2, jac, pp);
+      for (int i = 0; i < NV; ++i) o[i] = e ? kmath::nan() : pp[i];
     } else if (!strcmp(name, "krzysie_grid")) {
       // PUFFY 384x360 grid (koral/tests/golden/metric_golden_tests.zig:133)
       MetricParams mp = {0.0, 0.1, 0.9};

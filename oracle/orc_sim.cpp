@@ -1648,6 +1648,23 @@ int init_puffy(OSim& s, double perturb, double perturb_rho, uint64_t seed, doubl
   return e;
 }
 
+// A bare simulation of an nx x ny x nz grid with ng ghosts (extents
+// [minx, maxx] x ...): sizes and the zeroed arrays the per-function passes
+// below touch, with sqrt(-g) = 1 (the Minkowski grids of the reference's
+// flux_ct and calc_BfromA goldens).
+void bare_sim(OSim& s, int nx, int ny, int nz, int ng, const double ext[6]) {
+  s.g = grid_init(nx, ny, nz, ng, ext[0], ext[1], ext[2], ext[3], ext[4], ext[5]);
+  s.sx = nx + 2 * s.g.ngx;
+  s.sy = ny + 2 * s.g.ngy;
+  s.sz = nz + 2 * s.g.ngz;
+  s.nc = s.sx * s.sy * s.sz;
+  s.p.assign(s.nc * NV, 0.0);
+  s.vecpot.assign(s.nc * 6, 0.0);
+  s.cg.assign(s.nc * 20, 0.0);
+  for (long c = 0; c < s.nc; ++c) s.cg[c * 20 + 19] = 1.0;
+  for (int d = 0; d < 3; ++d) s.flb[d].init(s.g, d);
+}
+
 }  // namespace
 
 // ---- ctypes surface ----------------------------------------------------------
@@ -1865,5 +1882,45 @@ int orc_sim_get_array(void* h, int which, double* out) {
   }
   memcpy(out, v->data(), v->size() * 8);
   return (int)v->size();
+}
+
+// ct.fluxCt (koral/sim/ct.zig:38) on given face fluxes: fb[dim] holds the
+// B1, B2, B3 rows of the dim-direction face fluxes in the FaceStore layout
+// (koral/sim/storage.zig:62: one extra slice in its own dimension, ghosts
+// included, the three components fastest); rebuilt in place. NULL for an
+// inactive direction. The grid extents do not enter.
+int orc_flux_ct(int nx, int ny, int nz, int ng, double* fbx, double* fby, double* fbz) {
+  OSim s;
+  const double ext[6] = {0.0, 1.0, 0.0, 1.0, 0.0, 1.0};
+  bare_sim(s, nx, ny, nz, ng, ext);
+  double* fb[3] = {fbx, fby, fbz};
+  for (int d = 0; d < 3; ++d) {
+    if (!fb[d]) continue;
+    size_t nfc = s.flb[d].d.size() / NV;
+    for (size_t f = 0; f < nfc; ++f)
+      for (int k = 0; k < 3; ++k) s.flb[d].d[f * NV + B1 + k] = fb[d][f * 3 + k];
+  }
+  flux_ct(s);
+  for (int d = 0; d < 3; ++d) {
+    if (!fb[d]) continue;
+    size_t nfc = s.flb[d].d.size() / NV;
+    for (size_t f = 0; f < nfc; ++f)
+      for (int k = 0; k < 3; ++k) fb[d][f * 3 + k] = s.flb[d].d[f * NV + B1 + k];
+  }
+  return 0;
+}
+// calc_BfromA (koral/sim/ct.zig:184, overwrite) on a sqrt(-g) = 1 grid: A_i
+// of every cell, ghosts included (cell-major, 3 fastest, the Field order of
+// koral/field.zig), to B^i of the domain cells in the same layout (ghost
+// entries are zeroed, as the overwrite leaves them before set_bc).
+int orc_b_from_a(int nx, int ny, int nz, int ng, const double* ext, const double* a, double* b) {
+  OSim s;
+  bare_sim(s, nx, ny, nz, ng, ext);
+  for (long c = 0; c < s.nc; ++c)
+    for (int k = 0; k < 3; ++k) s.p[c * NV + B1 + k] = a[c * 3 + k];
+  curl_from_a(s, s.p, NV, B1);
+  for (long c = 0; c < s.nc; ++c)
+    for (int k = 0; k < 3; ++k) b[c * 3 + k] = s.vecpot[c * 6 + 3 + k];
+  return 0;
 }
 }

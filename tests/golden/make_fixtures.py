@@ -119,4 +119,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_fixtures.py <koral-zig checkout>")
+    main(sys.argv[1])

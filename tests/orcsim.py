@@ -65,6 +65,10 @@ def _bind():
     lib.orc_sim_kdmp_write.restype = ctypes.c_int
     lib.orc_sim_kdmp_load.argtypes = [vp, vp, ctypes.c_long, ctypes.POINTER(_kc.KcDumpHeader)]
     lib.orc_sim_kdmp_load.restype = ctypes.c_int
+    lib.orc_flux_ct.argtypes = [ctypes.c_int] * 4 + [vp] * 3
+    lib.orc_flux_ct.restype = ctypes.c_int
+    lib.orc_b_from_a.argtypes = [ctypes.c_int] * 4 + [vp] * 3
+    lib.orc_b_from_a.restype = ctypes.c_int
     lib.orc_options_puffy.argtypes = [ctypes.POINTER(KcOptions)]
     lib.orc_grid_puffy.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(KcGrid)]
     _sim_bound = True

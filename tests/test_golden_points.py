@@ -267,3 +267,61 @@ def test_corrected_christoffels_on_puffy_grid():
     t = DevTracker()
     t.add(o[:, 2:], z[:, 2:])
     t.check(1e-8, "kris-corrected mks2")
+
+
+def test_trans_pall_coco():
+    """koral/tests/golden/state_golden_tests.zig:94: MKS2 <-> KS and MKS2 <-> BL
+    primitive transforms, DevTracker bound 1e-10."""
+    i, o = load_kgld("state/frames_transpall")
+    z = run_golden("frames_transpall", i, 13)
+    t = DevTracker()
+    t.add(o, z)
+    t.check(1e-10, "trans_pall_coco")
+
+
+def _face_shape(nx, ny, nz, ng, dim):
+    sx, sy, sz = (n + 2 * ng if n > 1 else 1 for n in (nx, ny, nz))
+    return (sz + (dim == 2), sy + (dim == 1), sx + (dim == 0))
+
+
+def test_flux_ct():
+    """koral/tests/golden/step_golden_tests.zig:299-333: Minkowski periodic
+    32x32, the records' B rows of flbx/flby set, ct.fluxCt, bound 1e-15."""
+    from tests.orcsim import _bind
+
+    lib = _bind()
+    i, o = load_kgld("flux/ct")
+    nx, ny, nz, ng = 32, 32, 1, 3
+    fb = [np.zeros(_face_shape(nx, ny, nz, ng, d) + (3,)) for d in range(2)]
+    dims, ix, iy = i[:, 0].astype(int), i[:, 1].astype(int) + ng, i[:, 2].astype(int) + ng
+    for d in range(2):
+        m = dims == d
+        fb[d][0, iy[m], ix[m], :] = i[m, 3:6]
+    lib.orc_flux_ct(nx, ny, nz, ng, fb[0].ctypes.data, fb[1].ctypes.data, None)
+    got = np.array([fb[d][0, y, x, :] for d, x, y in zip(dims, ix, iy)])
+    t = DevTracker()
+    t.add(got, o)
+    t.check(1e-15, "flux_ct")
+
+
+def test_b_from_a():
+    """koral/tests/golden/step_golden_tests.zig:340-372: Minkowski periodic
+    32x32, A from the records, set_bc (periodic images in the ghosts),
+    calc_BfromA with overwrite, bound 1e-14."""
+    from tests.orcsim import _bind
+
+    lib = _bind()
+    i, o = load_kgld("flux/bfroma")
+    nx, ny, nz, ng = 32, 32, 1, 3
+    sx, sy = nx + 2 * ng, ny + 2 * ng
+    dom = np.zeros((ny, nx, 3))
+    dom[i[:, 1].astype(int), i[:, 0].astype(int)] = i[:, 2:5]
+    a = np.zeros((1, sy, sx, 3))
+    a[0] = dom[np.arange(-ng, ny + ng) % ny][:, np.arange(-ng, nx + ng) % nx]
+    b = np.zeros_like(a)
+    ext = np.array([0.0, 2 * np.pi, 0.0, 2 * np.pi, 0.0, 1.0])
+    lib.orc_b_from_a(nx, ny, nz, ng, ext.ctypes.data, a.ctypes.data, b.ctypes.data)
+    got = b[0, i[:, 1].astype(int) + ng, i[:, 0].astype(int) + ng]
+    t = DevTracker()
+    t.add(got, o)
+    t.check(1e-14, "calc_BfromA")

@@ -48,3 +48,18 @@ def test_noalloc_at_the_size_limit_and_beyond():
 
     st = lib.kc_implicit_batch_noalloc(ctypes.byref(opt), n + 1, None, None, None, None, 0)
     assert st == kc.KC_ERR_TOO_MANY_CELLS
+
+
+def test_noalloc_accepts_only_the_per_cell_form():
+    import ctypes
+
+    kc = koralcuda()
+    lib = kc.lib()
+    opt = kc.puffy_options()
+    geom, dt, pp = _records()
+    res = np.zeros((len(dt), 6), dtype=np.int32)
+    pw = pp.copy()
+    for mode in (kc.KC_IMPLICIT_COMPACTING, kc.KC_IMPLICIT_SORTED):
+        st = lib.kc_implicit_batch_noalloc(ctypes.byref(opt), len(dt), geom.ctypes.data, dt.ctypes.data,
+                                           pw.ctypes.data, res.ctypes.data, mode)
+        assert st == kc.KC_ERR_INVALID_CONFIG

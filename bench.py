@@ -316,9 +316,56 @@ def run_implicit(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+PRIM_NAMES = ["rho", "uu", "vx", "vy", "vz", "entr", "b1", "b2", "b3", "ee", "fx", "fy", "fz"]
+INTEGRATED = ("mass", "mdot", "radlum", "totallum", "scaleheight")
+
+
+def measure_forms(kc, grid, local, steps, seed, graph):
+    """The north-star forms on the benchmark's own wedge and init: plain FP64 and
+    the mixed form (KC_MIXED), each from a fresh init, the mixed run forced to the
+    plain run's dt sequence, timed with CUDA events on each engine's stream;
+    returns ms per step of both, the mixed form's per-primitive field-scale error
+    and the relative error of the integrated mass, accretion rate, luminosities
+    and scale height (dump.scalarRow) after the steps."""
+    import numpy as np
+    import torch
+
+    res, dts = {}, []
+    for form, mode in (("fp64", kc.KC_PLAIN_FP64), ("mixed", kc.KC_MIXED)):
+        sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode))
+        sim.initPuffy(1e-3, 1e-3, seed)
+        sim.set_graph(graph)
+        stream = torch.cuda.ExternalStream(sim.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for k in range(steps):
+            if form == "fp64":
+                dts.append(sim.step())
+            else:
+                sim.step(dts[k])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[form] = {"ms": e0.elapsed_time(e1) / steps, "p": sim.p, "scalars": sim.scalars(0.0, 5000.0, 15.0),
+                     "t": sim.counters()["t"]}
+        sim.close()
+    b, a = res["fp64"]["p"], res["mixed"]["p"]
+    ok = np.all(np.isfinite(b), axis=1)
+    dev = np.abs(a[ok] - b[ok]).max(axis=0) / np.maximum(np.abs(b[ok]).max(axis=0), 1e-300)
+    rel = {k: abs(res["mixed"]["scalars"][k] / res["fp64"]["scalars"][k] - 1) for k in INTEGRATED}
+    return {"steps": steps, "t": res["fp64"]["t"],
+            "plain_fp64_ms_per_step": res["fp64"]["ms"], "mixed_ms_per_step": res["mixed"]["ms"],
+            "mixed_speedup": res["fp64"]["ms"] / res["mixed"]["ms"],
+            "mixed_field_scale_error": dict(zip(PRIM_NAMES, dev.tolist())),
+            "mixed_integrated_rel_error": rel,
+            "note": "mixed = FP32 PPM on stencil deviations, FP32 LAXF dissipation, FP32 flux-CT; "
+                    "the rest FP64; same init and dt sequence as the plain run"}
+
+
 def run_precision(args, rank, local):
-    """The mixed form (FP32 reconstruction, LAXF, flux-CT) against plain FP64 on
-    the same wedge and init, the mixed run forced to the FP64 run's dt sequence:
+    """Mixed forms (FP32 reconstruction, LAXF, flux-CT, or any set of those pieces
+    and the rounded one-sided fluxes) against plain FP64 on the same wedge and
+    init, each mixed run forced to the FP64 run's dt sequence:
     per-primitive field-scale error of the final state and the relative error of
     the integrated mass, accretion rate (horizon), luminosity and scale height."""
     import numpy as np
@@ -330,7 +377,15 @@ def run_precision(args, rank, local):
     out = {}
     dts = []
     names = ["rho", "uu", "vx", "vy", "vz", "entr", "b1", "b2", "b3", "ee", "fx", "fy", "fz"]
-    for form, mode in (("fp64", 0), ("mixed", 1), ("fp64_seeded", 0)):
+    piece = {"all": kc.KC_MIXED, "ppm": kc.KC_FP32_PPM, "laxf": kc.KC_FP32_LAXF, "ct": kc.KC_FP32_CT,
+             "flux": kc.KC_FP32_FLUX}
+    variants = []
+    for name in args.mixed_forms.split(","):
+        mode = 0
+        for part in name.split("+"):
+            mode |= piece[part]
+        variants.append(("mixed" if name == "all" else "mixed_" + name, mode))
+    for form, mode in [("fp64", 0)] + variants + [("fp64_seeded", 0)]:
         sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode))
         sim.initPuffy(1e-3, 1e-3, args.seed)
         if form == "fp64_seeded":
@@ -363,14 +418,16 @@ def run_precision(args, rank, local):
              for k in ("mass", "mdot", "radlum", "totallum", "scaleheight")}
         return d, r
 
-    dev, rel = dev_of("mixed")
     dev_s, rel_s = dev_of("fp64_seeded")
     line = {"metric": METRIC, "unit": UNIT, "workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz}, {args.steps} steps",
             "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms_per_step"]},
-            "mixed": {"value": out["mixed"]["value"], "ms_per_step": out["mixed"]["ms_per_step"]},
-            "field_scale_error": dict(zip(names, dev.tolist())), "integrated_rel_error": rel,
             "fp64_seed_1e-15": {"field_scale": dict(zip(names, dev_s.tolist())), "integrated_rel": rel_s},
-            "scalars_fp64": out["fp64"]["scalars"], "scalars_mixed": out["mixed"]["scalars"]}
+            "scalars_fp64": out["fp64"]["scalars"]}
+    for form, mode in variants:
+        dev, rel = dev_of(form)
+        line[form] = {"precision_mode": mode, "value": out[form]["value"], "ms_per_step": out[form]["ms_per_step"],
+                      "field_scale_error": dict(zip(names, dev.tolist())), "integrated_rel_error": rel,
+                      "scalars": out[form]["scalars"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -482,6 +539,11 @@ def main():
                     help="launch the step's kernels eagerly instead of replaying a captured CUDA graph")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="skip the autotuner (implicit form and block sizes) before the timed steps")
+    ap.add_argument("--no-forms", dest="forms", action="store_false",
+                    help="skip the mixed-vs-plain comparison of the default workload")
+    ap.add_argument("--mixed-forms", default="all",
+                    help="precision workload: comma-separated FP32 piece sets (all, ppm, laxf, ct, flux, "
+                         "or a+b combinations) run beside plain FP64")
     ap.add_argument("--pairs", type=int, default=1000000, help="training pairs of the guess workload")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
@@ -612,6 +674,11 @@ def main():
     e2e = {"value": job_rate(ncell, ke, world, ems), "unit": UNIT, "h2d_bytes_per_step": e2e_bytes,
            "d2h_bytes_per_step": e2e_bytes, "steps": ke}
 
+    # ---- the mixed form beside plain FP64 (the metric's "at stated error") ----------
+    forms = None
+    if world == 1 and args.forms:
+        forms = measure_forms(kc, grid, local, args.steps, args.seed, args.graph)
+
     # ---- roofline of the dominant pass ---------------------------------------------
     peaks, peak_kind = measured_peaks()
     total = sum(v[0] for v in passes.values())
@@ -664,6 +731,8 @@ def main():
                    "pass_table": "timed region" if not args.graph else f"{pass_steps} eager steps after it"},
         "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": launches,
     }
+    if forms is not None:
+        line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, n, t = oracle_rate(args.nx, args.ny, SAMPLE_NZ, 1, 1, threads, min_seconds=10.0)

@@ -26,8 +26,19 @@ KC_HD Faces recon_linear(const double u[5], double theta) {
 
 KC_HD double my_sign_pm(double x) { return (x >= 0.0) ? 1.0 : -1.0; }
 
-// PPM with non-uniform widths, C finite.c:210 (recon.zig:107)
-KC_HD Faces recon_ppm(const double u[5], const double dx[5]) {
+// PPM with non-uniform widths, C finite.c:210 (recon.zig:107). The factors
+// that depend only on the five cell widths are formed once per stencil
+// position (ppm_coef) and shared by every variable reconstructed there
+// (ppm_apply). Each factor is a leading sub-product of the reference's
+// left-to-right expressions, so the split gives the one-piece routine's bits.
+struct PpmCoef {
+  double a, b, c;     // dri   = a * (b * (u3 - u2) + c * (u2 - u1))
+  double d, e, f;     // drip1 = d * (e * (u4 - u3) + f * (u3 - u2))
+  double g, h, i;     // drim1 = g * (h * (u2 - u1) + i * (u1 - u0))
+  double rm, rj, rk, rl, r_inv;  // right face
+  double lm, lj, lk, ll, l_inv;  // left face
+};
+KC_HD PpmCoef ppm_coef(const double dx[5]) {
   double dxm2 = dx[0], dxm1 = dx[1], dx0 = dx[2], dxp1 = dx[3], dxp2 = dx[4];
   double dxp2_plus_dxp1 = dxp2 + dxp1;
   double dxp2_plus_dxp1_inv = 1.0 / dxp2_plus_dxp1;
@@ -46,13 +57,36 @@ KC_HD Faces recon_ppm(const double u[5], const double dx[5]) {
   double twodxp1_plus_dx0 = 2.0 * dxp1 + dx0;
   double twodxp2_plus_dxp1 = 2.0 * dxp2 + dxp1;
   double twodx0_plus_dxm1 = 2.0 * dx0 + dxm1;
-
-  double dri = dx0 * dxm1_plus_dx0_plus_dxp1_inv *
-               (dx0_plus_twodxm1 * dxp1_plus_dx0_inv * (u[3] - u[2]) + twodxp1_plus_dx0 * dx0_plus_dxm1_inv * (u[2] - u[1]));
-  double drip1 = dxp1 * dx0_plus_dxp1_plus_dxp2_inv *
-                 (dxp1_plus_twodx0 * dxp2_plus_dxp1_inv * (u[4] - u[3]) + twodxp2_plus_dxp1 * dxp1_plus_dx0_inv * (u[3] - u[2]));
-  double drim1 = dxm1 * dxm2_plus_dxm1_plus_dx0_inv *
-                 (dxm1_plus_twodxm2 * dx0_plus_dxm1_inv * (u[2] - u[1]) + twodx0_plus_dxm1 * dxm1_plus_dxm2_inv * (u[1] - u[0]));
+  PpmCoef k;
+  k.a = dx0 * dxm1_plus_dx0_plus_dxp1_inv;
+  k.b = dx0_plus_twodxm1 * dxp1_plus_dx0_inv;
+  k.c = twodxp1_plus_dx0 * dx0_plus_dxm1_inv;
+  k.d = dxp1 * dx0_plus_dxp1_plus_dxp2_inv;
+  k.e = dxp1_plus_twodx0 * dxp2_plus_dxp1_inv;
+  k.f = twodxp2_plus_dxp1 * dxp1_plus_dx0_inv;
+  k.g = dxm1 * dxm2_plus_dxm1_plus_dx0_inv;
+  k.h = dxm1_plus_twodxm2 * dx0_plus_dxm1_inv;
+  k.i = twodx0_plus_dxm1 * dxm1_plus_dxm2_inv;
+  double z1 = dx0_plus_dxm1 / dxp1_plus_twodx0;
+  double z2 = dxp2_plus_dxp1 / twodxp1_plus_dx0;
+  k.r_inv = 1.0 / (dxm1 + dx0 + dxp1 + dxp2);
+  k.rm = dx0 * dxp1_plus_dx0_inv;
+  k.rj = (2.0 * dxp1 * dx0) * dxp1_plus_dx0_inv * (z1 - z2);
+  k.rk = dx0 * z1;
+  k.rl = dxp1 * z2;
+  z1 = dxm1_plus_dxm2 / dx0_plus_twodxm1;
+  z2 = dxp1_plus_dx0 / twodx0_plus_dxm1;
+  k.l_inv = 1.0 / (dxm2 + dxm1 + dx0 + dxp1);
+  k.lm = dxm1 * dx0_plus_dxm1_inv;
+  k.lj = (2.0 * dx0 * dxm1) * dx0_plus_dxm1_inv * (z1 - z2);
+  k.lk = dxm1 * z1;
+  k.ll = dx0 * z2;
+  return k;
+}
+KC_HD Faces ppm_apply(const double u[5], const PpmCoef& k) {
+  double dri = k.a * (k.b * (u[3] - u[2]) + k.c * (u[2] - u[1]));
+  double drip1 = k.d * (k.e * (u[4] - u[3]) + k.f * (u[3] - u[2]));
+  double drim1 = k.g * (k.h * (u[2] - u[1]) + k.i * (u[1] - u[0]));
 
   dri = ((u[3] - u[2]) * (u[2] - u[1]) > 0.0)
             ? kmath::fmin(kmath::fabs(dri),
@@ -67,18 +101,8 @@ KC_HD Faces recon_ppm(const double u[5], const double dx[5]) {
                             kmath::fmin(2.0 * kmath::fabs(u[1] - u[0]), 2.0 * kmath::fabs(u[1] - u[2]))) * my_sign_pm(drim1)
               : 0.0;
 
-  double z1 = dx0_plus_dxm1 / dxp1_plus_twodx0;
-  double z2 = dxp2_plus_dxp1 / twodxp1_plus_dx0;
-  double dx_inv = 1.0 / (dxm1 + dx0 + dxp1 + dxp2);
-  double right = u[2] + dx0 * dxp1_plus_dx0_inv * (u[3] - u[2]) +
-                 dx_inv * ((2.0 * dxp1 * dx0) * dxp1_plus_dx0_inv * (z1 - z2) * (u[3] - u[2]) - dx0 * z1 * drip1 +
-                           dxp1 * z2 * dri);
-  z1 = dxm1_plus_dxm2 / dx0_plus_twodxm1;
-  z2 = dxp1_plus_dx0 / twodx0_plus_dxm1;
-  dx_inv = 1.0 / (dxm2 + dxm1 + dx0 + dxp1);
-  double left = u[1] + dxm1 * dx0_plus_dxm1_inv * (u[2] - u[1]) +
-                dx_inv * ((2.0 * dx0 * dxm1) * dx0_plus_dxm1_inv * (z1 - z2) * (u[2] - u[1]) - dxm1 * z1 * dri +
-                          dx0 * z2 * drim1);
+  double right = u[2] + k.rm * (u[3] - u[2]) + k.r_inv * (k.rj * (u[3] - u[2]) - k.rk * drip1 + k.rl * dri);
+  double left = u[1] + k.lm * (u[2] - u[1]) + k.l_inv * (k.lj * (u[2] - u[1]) - k.lk * dri + k.ll * drim1);
 
   bool flat = (right - u[2]) * (u[2] - left) <= 0.0;
   if (flat) {
@@ -92,6 +116,7 @@ KC_HD Faces recon_ppm(const double u[5], const double dx[5]) {
   f.right = right;
   return f;
 }
+KC_HD Faces recon_ppm(const double u[5], const double dx[5]) { return ppm_apply(u, ppm_coef(dx)); }
 
 enum : int { RECON_DONOR = 0, RECON_LINEAR = 1, RECON_PPM = 2 };
 KC_HD Faces reconstruct(int scheme, const double u[5], const double dx[5], double theta) {

@@ -117,9 +117,11 @@ KC_HDN int apply_constraints(double pp[NV], double uu[NV], const double uu0[NV],
 
 // C f_implicit_lab_4dprim_with_state (implicit.zig:337); returns the max
 // normalized error (NaN entries never win the max, as in the reference).
+// `opdamp` is the ladder level's opacity damping (radforce.Params.opdamp,
+// carried apart from `op` so the level's parameters are never copied).
 KC_HDN double implicit_residual(const double uu[NV], const double pp[NV], const RadState& st, const double uu0[NV],
-                                const RadState& st0, double dt, const Geom& g, const OpacParams& op, int whichprim,
-                                int whicheq, int whichframe, double f[4]) {
+                                const RadState& st0, double dt, const Geom& g, const OpacParams& op, double opdamp,
+                                int whichprim, int whicheq, int whichframe, double f[4]) {
   const double small = 1.0e-80;
   double gdetu = g.gdet;
   double tgas = st.tgas;
@@ -127,7 +129,8 @@ KC_HDN double implicit_residual(const double uu[NV], const double pp[NV], const 
   double ehat = st.ehat;
   double dtau = kmath::div(dt, st.ucon[0]);
   double giff[4], gilab[4], gi[4];
-  calc_gi_from_state(st, pp[VX], pp[VY], pp[VZ], g, op, false, giff, gilab);
+  calc_gi_undamped(st, pp[VX], pp[VY], pp[VZ], g, op, false, giff, gilab);
+  damp_gi(opdamp, giff, gilab);
   lower_vec(gilab, g, gi);
   double err[4] = {0.0, 0.0, 0.0, 0.0};
   if (whichprim == PRIM_MHD) {
@@ -303,8 +306,9 @@ KC_HD void lag_opac(RadState& st, const RadState& st00) {
 // C solve_implicit_lab_4dprim Newton core (implicit.zig:642). Returns 1 on
 // success (pp_out written, *iters set), 0 on failure.
 KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, const double pp0in[NV], const Geom& g,
-                             double dt, double gam, const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
-                             int whichprim, int whicheq, int whichframe, double pp_out[NV], int* iters_out) {
+                             double dt, double gam, const RadParams& rad, const OpacParams& op, double opdamp,
+                             const ImplicitParams& ip, int whichprim, int whicheq, int whichframe, double pp_out[NV],
+                             int* iters_out) {
   double uu[NV], pp[NV];
   for (int i = 0; i < NV; ++i) {
     uu[i] = uu00[i];
@@ -327,7 +331,7 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
     for (int i = 0; i < NV; ++i) ppp[i] = pp[i];
     double xxx[4];
     if (fret < -1) return 0;
-    double errbase = implicit_residual(uu, pp, state, uu00, state00, dt, g, op, whichprim, whicheq, whichframe, f1);
+    double errbase = implicit_residual(uu, pp, state, uu00, state00, dt, g, op, opdamp, whichprim, whicheq, whichframe, f1);
     if (errbase < conv) {
       success = true;
       break;
@@ -350,7 +354,7 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
         }
         fill_rad_state(pp, g, gam, op, !slim, state);
         if (ip.lag_opac) lag_opac(state, state00);
-        implicit_residual(uu, pp, state, uu00, state00, dt, g, op, whichprim, whicheq, whichframe, f2);
+        implicit_residual(uu, pp, state, uu00, state00, dt, g, op, opdamp, whichprim, whicheq, whichframe, f2);
         for (int i = 0; i < 4; ++i) jac[i][j] = kmath::div((f2[i] - f1[i]), del);
         pp[j + sh] = ppp[j + sh];
         break;
@@ -483,17 +487,15 @@ KC_HDN ImplicitResult implicit_ladder(double uu[NV], double pp[NV], const Geom& 
   res.whicheq = EQ_ENERGY;
   res.whichframe = FRAME_LAB;
   for (int level = 0; level <= ip.opdamp_maxlevels; ++level) {
-    OpacParams opl = op;
-    double od = 1.0;
+    double od = 1.0;  // the level's opdamp (implicit.zig:955)
     for (int i = 0; i < level; ++i) od /= ip.opdamp_factor;
-    opl.opdamp = od;
     KC_ROLLED
     for (int ir = 0; ir < 6; ++ir) {
       int p, e, fr;
       implicit_rung(ir, pre.startwith, p, e, fr);
       double ppw[NV];
       int iters = 0;
-      if (solve_4dprim_core(pre.uu00, pre.state00, pre.pp0, g, dt, gam, rad, opl, ip, p, e, fr, ppw, &iters)) {
+      if (solve_4dprim_core(pre.uu00, pre.state00, pre.pp0, g, dt, gam, rad, op, od, ip, p, e, fr, ppw, &iters)) {
         for (int i = 0; i < NV; ++i) pp[i] = ppw[i];
         p2u(ppw, uu, g, gam);
         res.ok = 1;
@@ -524,7 +526,8 @@ KC_HDN ImplicitResult solve_implicit_lab(double uu[NV], double pp[NV], const Geo
 // reject the start.
 KC_HD double implicit_start_residual(const double uu00[NV], const RadState& state00, const double start[NV],
                                      const Geom& g, double dt, double gam, const RadParams& rad,
-                                     const OpacParams& op, const ImplicitParams& ip, int whichprim, double pp[NV]) {
+                                     const OpacParams& op, double opdamp, const ImplicitParams& ip, int whichprim,
+                                     double pp[NV]) {
   double uu[NV], f[4];
   for (int i = 0; i < NV; ++i) {
     uu[i] = uu00[i];
@@ -534,7 +537,7 @@ KC_HD double implicit_start_residual(const double uu00[NV], const RadState& stat
   RadState st;
   fill_rad_state(pp, g, gam, op, false, st);
   if (ip.lag_opac) lag_opac(st, state00);
-  return implicit_residual(uu, pp, st, uu00, state00, dt, g, op, whichprim, EQ_ENERGY, FRAME_LAB, f);
+  return implicit_residual(uu, pp, st, uu00, state00, dt, g, op, opdamp, whichprim, EQ_ENERGY, FRAME_LAB, f);
 }
 
 // The opening of rung 0 of the ladder (level 0, start fluid, energy equation,
@@ -546,12 +549,10 @@ KC_HD double implicit_start_residual(const double uu00[NV], const RadState& stat
 KC_HDN int implicit_first_exit(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
                                const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
                                const ImplicitPre& pre) {
-  OpacParams opl = op;
-  opl.opdamp = 1.0;
   int p, e, fr;
   implicit_rung(0, pre.startwith, p, e, fr);
   double pc[NV];
-  double e0 = implicit_start_residual(pre.uu00, pre.state00, pre.pp0, g, dt, gam, rad, opl, ip, p, pc);
+  double e0 = implicit_start_residual(pre.uu00, pre.state00, pre.pp0, g, dt, gam, rad, op, 1.0, ip, p, pc);
   if (!(e0 < ip.conv)) return 0;
   for (int i = 0; i < NV; ++i) pp[i] = pc[i];
   p2u(pc, uu, g, gam);
@@ -576,10 +577,8 @@ KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], cons
   double ehat = -calc_ff_rtt(pp, g, nullptr);
   fill_rad_state(pp, g, gam, op, true, pre.state00);
   pre.startwith = (ehat < ip.threshold * pp[UU]) ? PRIM_RAD : PRIM_MHD;
-  OpacParams opl = op;
-  opl.opdamp = 1.0;
   double pc[NV];
-  double e0 = implicit_start_residual(pre.uu00, pre.state00, pp, g, dt, gam, rad, opl, ip, pre.startwith, pc);
+  double e0 = implicit_start_residual(pre.uu00, pre.state00, pp, g, dt, gam, rad, op, 1.0, ip, pre.startwith, pc);
   if (e0 < ip.conv) {
     // the core's first exit on rung 0 (lab frame, energy equation)
     ImplicitResult res;
@@ -593,7 +592,7 @@ KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], cons
     res.whichframe = FRAME_LAB;
     return res;
   }
-  double e1 = implicit_start_residual(pre.uu00, pre.state00, guess, g, dt, gam, rad, opl, ip, pre.startwith, pc);
+  double e1 = implicit_start_residual(pre.uu00, pre.state00, guess, g, dt, gam, rad, op, 1.0, ip, pre.startwith, pc);
   bool learned = e1 < e0;
   for (int i = 0; i < NV; ++i) pre.pp0[i] = learned ? guess[i] : pp[i];
   return implicit_ladder(uu, pp, g, dt, gam, rad, op, ip, pre);

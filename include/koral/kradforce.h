@@ -332,10 +332,11 @@ KC_HD double compton_gi_coeff(const Consts& c, const RadState& st) {
   return kmath::div(st.kappaes * st.ehat * ((4.0 * c.kb_over_me) * (st.trad - st.te)) *
          (1.0 + 3.683 * thetae + 4.0 * thetae * thetae), (1.0 + 4.0 * thetae));
 }
-// C calc_all_Gi_with_state thermal part (radforce.zig:432). full=false leaves
-// ff[1..3] zero and skips the boost (the solver path).
-KC_HDM void calc_gi_from_state(const RadState& st, double v1, double v2, double v3, const Geom& g, const OpacParams& op,
-                              bool full, double gi_ff[4], double gi_lab[4]) {
+// C calc_all_Gi_with_state thermal part (radforce.zig:432) before the
+// opacity-damping factor. full=false leaves ff[1..3] zero and skips the boost
+// (the solver path).
+KC_HDM void calc_gi_undamped(const RadState& st, double v1, double v2, double v3, const Geom& g, const OpacParams& op,
+                             bool full, double gi_ff[4], double gi_lab[4]) {
   const Consts& c = op.c;
   double b = c.sigma_rad_over_pi * st.te * st.te * st.te * st.te;
   double k_rad_abs = st.opac.rad_abs, k_gas_abs = st.opac.gas_abs, k_rad_ross = st.opac.rad_ross;
@@ -357,13 +358,21 @@ KC_HDM void calc_gi_from_state(const RadState& st, double v1, double v2, double 
     for (int i = 0; i < 4; ++i) gi_lab[i] += coeff * st.ucon[i];
     gi_ff[0] += coeff;
   }
-  if (op.opdamp != 1.0) {
-    double od = op.opdamp;
+}
+// the opacity-damping factor of the implicit ladder's damped levels
+KC_HD void damp_gi(double od, double gi_ff[4], double gi_lab[4]) {
+  if (od != 1.0) {
     for (int i = 0; i < 4; ++i) {
       gi_ff[i] *= od;
       gi_lab[i] *= od;
     }
   }
+}
+// C calc_all_Gi_with_state thermal part (radforce.zig:432), damped by op.opdamp
+KC_HDM void calc_gi_from_state(const RadState& st, double v1, double v2, double v3, const Geom& g, const OpacParams& op,
+                              bool full, double gi_ff[4], double gi_lab[4]) {
+  calc_gi_undamped(st, v1, v2, v3, g, op, full, gi_ff, gi_lab);
+  damp_gi(op.opdamp, gi_ff, gi_lab);
 }
 
 // C calc_kappaes standalone flavor, Trad = Te (radforce.zig:522)

@@ -50,6 +50,13 @@ enum {
 
 enum { KC_BC_PERIODIC = 0, KC_BC_COPY = 1, KC_BC_PUFFY = 2 };
 enum { KC_PLAIN_FP64 = 0, KC_MIXED = 1 };
+/* The FP32 pieces of the mixed form, which kc_set_precision also takes one by
+ * one or combined (no reference counterpart): the PPM reconstruction on
+ * stencil deviations, the LAXF dissipation product, the flux-CT corner
+ * averages, and the one-sided face fluxes rounded to FP32 (their arithmetic
+ * stays FP64: the rounding alone bounds what FP32 flux arithmetic would do).
+ * KC_MIXED is KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_CT. */
+enum { KC_FP32_PPM = 2, KC_FP32_LAXF = 4, KC_FP32_CT = 8, KC_FP32_FLUX = 16 };
 enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
 /* implicit pass forms (no reference counterpart; all bit-identical to the
  * reference's per-cell solveImplicitLab loop, koral/sim.zig:1715):
@@ -126,7 +133,7 @@ typedef struct kc_options {
   int32_t reduceorderatbh, reduceorderafterfixup, dampradwavespeednearaxis;
   int32_t bc_x, bc_y, bc_z;
   /* engine forms (no reference counterpart) */
-  int32_t precision;     /* KC_PLAIN_FP64 | KC_MIXED */
+  int32_t precision;     /* KC_PLAIN_FP64, KC_MIXED, or a set of KC_FP32_* pieces */
   int32_t implicit_mode; /* KC_IMPLICIT_PER_CELL | KC_IMPLICIT_COMPACTING | KC_IMPLICIT_SPLIT */
   int32_t device;        /* CUDA device ordinal */
 } kc_options;
@@ -251,13 +258,16 @@ int kc_set_graph(kc_handle* h, int32_t on);
  * per-cell implicit, face-flux and u2p kernels, and the per-cell implicit
  * kernel's thread -> cell order (1, the default: phi fastest on 3D grids, so
  * that a warp's cells share r and theta, theta fastest on 2D grids; 0: x
- * fastest), with the measured step time of the choice and of the
- * configuration on entry. */
+ * fastest) and its register budget (resident blocks of 128 threads per SM: 2
+ * with 255 registers per thread, 3 with 168), with the measured step time of
+ * the choice and of the configuration on entry. */
 typedef struct kc_tune_result {
   int32_t implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
   double ms_per_step, ms_per_step_entry;
   int32_t trials;
   int32_t implicit_phi_fastest;
+  int32_t implicit_min_blocks; /* 2: 255 registers per thread, 3: 168; 0: by cell order */
+  int32_t reserved;
 } kc_tune_result;
 /* Times whole steps on the handle's current state for each candidate, one
  * knob at a time, and keeps the fastest configuration set; the state and the
@@ -385,6 +395,16 @@ int kc_synth_implicit_cells(const kc_options* opt, int64_t n, uint64_t seed, dou
 #define KC_NOALLOC_MAX_CELLS 16384
 int kc_implicit_batch_noalloc(const kc_options* opt, int64_t n, const double* geom23, const double* dt, double* pp,
                               int32_t* res, int32_t mode);
+/* ct.fluxCt (koral/sim/ct.zig:38-177) on given face fluxes, without a handle,
+ * on `device`: fb_x/fb_y/fb_z hold the B1, B2, B3 rows of the x/y/z face
+ * fluxes of an nx x ny x nz domain with ng ghost layers, in the reference's
+ * FaceStore layout (koral/sim/storage.zig:62: the face direction has one more
+ * slice, ghosts included, offset = ((jz*FY + jy)*FX + jx)*3 + k with
+ * FX = SX + (dir == x) etc.); the corner EMFs are formed and the B rows
+ * rebuilt in place, as the step's flux-CT pass does. An inactive direction's
+ * array may be NULL. */
+int kc_flux_ct(int32_t device, int32_t nx, int32_t ny, int32_t nz, int32_t ng, double* fb_x, double* fb_y,
+               double* fb_z);
 /* u2p cascade of one cell as calcU2p applies it (koral/sim.zig:972-994):
  * u2pMhd + u2pRad + both floors. flags_out: {entropy_used, hd_fixup, rad_fixup} */
 int kc_u2p_batch(const kc_options* opt, int64_t n, const double* geom23, const double* uu, double* pp,

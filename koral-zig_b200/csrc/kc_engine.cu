@@ -76,6 +76,9 @@ struct kc_handle {
   // phi fastest (warps of cells sharing r and theta) or x fastest; for the
   // implicit kernel on 2D grids the same switch selects theta fastest
   int implicit_phi_fastest = KC_IMPLICIT_PHI_FASTEST, u2p_phi_fastest = KC_U2P_PHI_FASTEST;
+  // resident blocks of 128 per SM the per-cell implicit kernel's registers allow:
+  // 2 (255 registers) or 3 (168); 0 picks by cell order (2 when phi is fastest)
+  int implicit_min_blocks = 0;
   // the step's dt-derived coefficients: pinned host table and its device copy
   // (DevState::coef); slots 0-3 are fixed by run_step, later ones appended
   double* coef_host = nullptr;
@@ -385,6 +388,11 @@ int ensure_split(kc_handle* h) {
   return KC_OK;
 }
 
+int implicit_blocks(const kc_handle* h, const ImplArgs& a) {
+  if (h->implicit_min_blocks) return h->implicit_min_blocks;
+  return a.phi_fastest ? 2 : 3;
+}
+
 void launch_implicit(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   ImplArgs a;
@@ -446,7 +454,7 @@ void launch_implicit(kc_handle* h, int dt_slot) {
   ++h->n_launch;
   unsigned nb = nblk(ndom, h->tpb_implicit);
   if (extra) k_implicit<true, 2><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
-  else if (a.phi_fastest) k_implicit<false, 2><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  else if (implicit_blocks(h, a) == 2) k_implicit<false, 2><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
   else k_implicit<false, 3><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
 }
 
@@ -463,6 +471,12 @@ void launch_wavespeeds(kc_handle* h) {
   k_wavespeeds<<<nblk(n), TPB, 0, h->stream>>>(h->ds, h->dsc, a);
 }
 
+// the FP32 pieces a precision mode selects (KC_MIXED: PPM, LAXF and CT)
+int fp32_pieces(int precision) {
+  if (precision == KC_MIXED) return KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_CT;
+  return precision & (KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_CT | KC_FP32_FLUX);
+}
+
 void launch_face_fluxes(kc_handle* h) {
   const DGrid& gr = h->gr;
   FluxArgs a;
@@ -471,6 +485,7 @@ void launch_face_fluxes(kc_handle* h) {
   a.maxvel = h->sp.maxradviscvel;
   a.fl = h->sp.fl;
   a.radvisc = h->sp.radviscosity;
+  a.fp32 = fp32_pieces(h->opt.precision);
   long dims[3] = {gr.nx, gr.ny, gr.nz};
   PassScope ps(h, KC_PASS_FLUXES);
   for (int d = 0; d < 3; ++d) cudaMemsetAsync(h->ds.flb[d], 0, (size_t)NV * h->ds.nf[d] * 8, h->stream);
@@ -483,7 +498,7 @@ void launch_face_fluxes(kc_handle* h) {
     ++h->n_launch;
     int tb = h->tpb_flux;
     unsigned nb = nblk(n, tb);
-    bool mx = h->opt.precision == KC_MIXED;
+    bool mx = (a.fp32 & (KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_FLUX)) != 0;
     if (dim == 0) {
       if (mx) k_face_flux<true, 0><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
       else k_face_flux<false, 0><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
@@ -502,10 +517,11 @@ void launch_flux_ct(kc_handle* h) {
   long n = (long)(gr.nx + 1) * (gr.ny + 1) * (gr.nz + 1);
   PassScope ps(h, KC_PASS_FLUXCT);
   ++h->n_launch;
-  if (h->opt.precision == KC_MIXED) k_ct_emf<float><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  const bool ct32 = (fp32_pieces(h->opt.precision) & KC_FP32_CT) != 0;
+  if (ct32) k_ct_emf<float><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
   else k_ct_emf<double><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
   ++h->n_launch;
-  if (h->opt.precision == KC_MIXED) k_ct_rebuild<float><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
+  if (ct32) k_ct_rebuild<float><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
   else k_ct_rebuild<double><<<nblk(n, 256), 256, 0, h->stream>>>(h->ds);
 }
 
@@ -1246,7 +1262,9 @@ int kc_debug_get_array(kc_handle* h, int which, double* out) {
 
 int kc_set_precision(kc_handle* h, int32_t mode) {
   if (!h) return KC_ERR_INVALID_CONFIG;
-  if (mode != KC_PLAIN_FP64 && mode != KC_MIXED) return reject(h, KC_ERR_INVALID_CONFIG, "unknown precision mode");
+  const int pieces = KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_CT | KC_FP32_FLUX;
+  if (mode != KC_PLAIN_FP64 && mode != KC_MIXED && (mode & ~pieces) != 0)
+    return reject(h, KC_ERR_INVALID_CONFIG, "unknown precision mode");
   h->opt.precision = mode;
   drop_graph(h);
   return KC_OK;

@@ -83,13 +83,6 @@ struct ImpLane {
   int ok, rung, iters;
 };
 
-// opacities of the current rung's damping level (implicit.zig:963)
-__device__ __forceinline__ OpacParams rung_opac(const ImpLane& L, const ImpParams& P) {
-  OpacParams o = P.op;
-  o.opdamp = L.od;
-  return o;
-}
-
 // the f1d_err state at L.b_x (implicit.zig:431): the trial pp into L.pp
 __device__ __forceinline__ void f1d_setup(ImpLane& L) {
   double ugas, ehat;
@@ -107,15 +100,13 @@ __device__ __forceinline__ void f1d_setup(ImpLane& L) {
 
 // The warp-wide evaluation: one call site for every lane's expensive work.
 __device__ __noinline__ void imp_eval(ImpLane& L, int kind, const ImpParams& P) {
-  OpacParams opl = rung_opac(L, P);
   if (kind == EV_CF || kind == EV_FD) L.fret = apply_constraints(L.pp, L.uu, L.uu00, L.g, P.gam, P.rp, P.ip, L.p);
   bool gated = kind == EV_FD && L.fret < -1;
   if (kind != EV_NONE && kind != EV_R && !gated) {
     bool full = kind == EV_FILL00 || ((kind == EV_CF || kind == EV_FD) && !L.slim);
     const double* src = kind == EV_FILL00 ? L.pp00 : L.pp;
     RadState& dst = kind == EV_FILL00 ? L.state00 : L.state;
-    const OpacParams& ox = (kind == EV_FILL00 || kind == EV_F1D) ? P.op : opl;
-    fill_rad_state(src, L.g, P.gam, ox, full, dst);
+    fill_rad_state(src, L.g, P.gam, P.op, full, dst);  // the state fill does not read the damping
     if ((kind == EV_CF || kind == EV_FD) && P.ip.lag_opac) lag_opac(L.state, L.state00);
   }
   if (kind == EV_F1D) {
@@ -126,7 +117,7 @@ __device__ __noinline__ void imp_eval(ImpLane& L, int kind, const ImpParams& P) 
     else L.b_val = L.b_x - L.pp00[UU] - L.b_dtau * giff[0];
   }
   if (kind == EV_R || (kind == EV_FD && !gated))
-    L.errx = implicit_residual(L.uu, L.pp, L.state, L.uu00, L.state00, L.dt, L.g, opl, L.p, L.e, L.fr,
+    L.errx = implicit_residual(L.uu, L.pp, L.state, L.uu00, L.state00, L.dt, L.g, P.op, L.od, L.p, L.e, L.fr,
                                kind == EV_R ? L.f1 : L.f2);
 }
 

@@ -263,7 +263,8 @@ __global__ void __launch_bounds__(128) k_update_entropy(DevState s, double gam) 
 }
 
 // ---- u2p (koral/sim.zig:924-1000) --------------------------------------------
-__global__ void __launch_bounds__(128, KC_U2P_MIN_BLOCKS) k_u2p(DevState s, DevScalars* sc, double gam, FloorParams fl, RadParams rp,
+__global__ void __launch_bounds__(128, KC_U2P_MIN_BLOCKS) k_u2p(DevState s, DevScalars* sc, double gam, const __grid_constant__ FloorParams fl,
+                                             const __grid_constant__ RadParams rp,
                                              int polar_nc, int phi_fastest) {
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
@@ -709,7 +710,7 @@ struct WsArgs {
   OpacParams op;
   int damp_nc;
 };
-__global__ void __launch_bounds__(128) k_wavespeeds(DevState s, DevScalars* sc, WsArgs a) {
+__global__ void __launch_bounds__(128) k_wavespeeds(DevState s, DevScalars* sc, const __grid_constant__ WsArgs a) {
   const Grid& g = s.gr.g;
   bool act[3] = {s.gr.nx > 1, s.gr.ny > 1, s.gr.nz > 1};
   long lx = act[0], ly = act[1], lz = act[2];
@@ -797,6 +798,7 @@ struct FluxArgs {
   double gam, theta, maxvel;
   FloorParams fl;
   int radvisc;
+  int fp32;  // the mixed instance's FP32 pieces (KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_FLUX)
 };
 __device__ __forceinline__ void face_rijvisc(const DevState& s, long c, long cm, double rv[4][4]) {
   long nc = s.gr.nc;
@@ -811,6 +813,8 @@ __device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, 
   if (gc) atomicAdd(&sc->n_guard, (unsigned long long)gc);
   int e = f_flux_prime(pp, dim, g, a.gam, ff);
   if (e) return e;
+  if (a.fp32 & KC_FP32_FLUX)
+    for (int iv = 0; iv < NV; ++iv) ff[iv] = (double)(float)ff[iv];
   p2u(pp, uu, g, a.gam);
   if (a.radvisc) {
     double rv[4][4];
@@ -824,11 +828,12 @@ __device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, 
 // 3 caps it at 168 registers (194 uncapped), measured 14% faster; 4 (128) 10%
 #define KC_FLUX_MIN_BLOCKS 3
 #endif
-// MIXED: the reconstruction and the LAXF combination in FP32 (kc_mixed.cuh)
+// MIXED: the instance of the mixed form, whose FP32 pieces (reconstruction,
+// LAXF dissipation, rounded fluxes; kc_mixed.cuh) FluxArgs::fp32 selects
 // DIM: the face direction, a template argument so that every index along it
 // is a compile-time one (one instance per direction)
 template <bool MIXED, int DIM>
-__global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState s, DevScalars* sc, FluxArgs a) {
+__global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState s, DevScalars* sc, const __grid_constant__ FluxArgs a) {
   constexpr int dim = DIM;
   long n = dim == 0 ? s.gr.nx : dim == 1 ? s.gr.ny : s.gr.nz;
   int c0d = dim == 0 ? 1 : 0, c1d = dim == 2 ? 1 : 2;
@@ -867,17 +872,20 @@ __global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState 
   double dxs[6];
   for (int k = 0; k < 6; ++k) dxs[k] = cell_size(g, f - 3 + k, dim);
   double pL[NV], pR[NV];
+  PpmCoef kl, kr;  // the width factors of the two stencils, shared by the 13 variables
+  if (!MIXED || !(a.fp32 & KC_FP32_PPM)) {
+    kl = ppm_coef(dxs);
+    kr = ppm_coef(dxs + 1);
+  }
   for (int iv = 0; iv < NV; ++iv) {
     double v[6];
     for (int k = 0; k < 6; ++k) v[k] = s.p[iv * nc + cst[k]];
-    if (MIXED) {
+    if (MIXED && (a.fp32 & KC_FP32_PPM)) {
       pL[iv] = recon_ppm_mixed(v, dxs).right;
       pR[iv] = recon_ppm_mixed(v + 1, dxs + 1).left;
     } else {
-      Faces fl = reconstruct(RECON_PPM, v, dxs, a.theta);          // cell f-1: right face value
-      Faces fr = reconstruct(RECON_PPM, v + 1, dxs + 1, a.theta);  // cell f: left face value
-      pL[iv] = fl.right;
-      pR[iv] = fr.left;
+      pL[iv] = ppm_apply(v, kl).right;      // cell f-1: right face value
+      pR[iv] = ppm_apply(v + 1, kr).left;   // cell f: left face value
     }
   }
   Geom geo;
@@ -897,8 +905,8 @@ __global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState 
   long nfd = s.nf[dim];
 #pragma unroll
   for (int iv = 0; iv < NV; ++iv)
-    out[iv * nfd + fi] = MIXED ? laxf_f(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag)
-                               : laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
+    out[iv * nfd + fi] = (MIXED && (a.fp32 & KC_FP32_LAXF)) ? laxf_f(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag)
+                                                         : laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
 }
 
 // ---- flux-CT (koral/sim/ct.zig:38) --------------------------------------------
@@ -1039,7 +1047,8 @@ struct ImplExtra {
 // of 3D grids, whose warps walk the solver together, 255 registers measured 6%
 // faster than 168 and 128 slower still. The host picks the instance by order.
 template <bool EXTRA, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* sc, ImplArgs a, ImplExtra x) {
+__global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
+                                                            ImplExtra x) {
   const double dt = s.coef[a.dt_slot];
   long ix, iy, iz;
   if (a.phi_fastest) {
@@ -1115,7 +1124,8 @@ struct SplitList {
   double* pp0;                // [NV][capacity] warm starts
   long cap;
 };
-__global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* sc, ImplArgs a, SplitList L) {
+__global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
+                                                        SplitList L) {
   const double dt = s.coef[a.dt_slot];
   Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
   long ix, iy, iz;
@@ -1145,7 +1155,8 @@ __global__ void __launch_bounds__(128) k_implicit_open(DevState s, DevScalars* s
   L.cell[k] = (int)(ix + s.gr.nx * (iy + s.gr.ny * iz));
   for (int i = 0; i < NV; ++i) L.pp0[(long)i * L.cap + (long)k] = pre.pp0[i];
 }
-__global__ void __launch_bounds__(128) k_implicit_ladder(DevState s, DevScalars* sc, ImplArgs a, SplitList L) {
+__global__ void __launch_bounds__(128) k_implicit_ladder(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
+                                                          SplitList L) {
   const double dt = s.coef[a.dt_slot];
   long n = (long)*L.count;
   if (n > L.cap) n = L.cap;
@@ -1230,7 +1241,8 @@ __global__ void __launch_bounds__(128) k_mlp_forward(MlpDev m, long n, const flo
 }
 
 // the same operator as a persistent, lane-refilling state machine (bit-identical)
-__global__ void __launch_bounds__(128) k_implicit_persistent(DevState s, DevScalars* sc, ImplArgs a, long nwork) {
+__global__ void __launch_bounds__(128) k_implicit_persistent(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
+                                                              long nwork) {
   const double dt = s.coef[a.dt_slot];
   long nyb = s.gr.ny - 2L * a.polar_nc;
   ImpStepSrc src{s, sc, dt, s.gr.nx, nyb, (long)a.polar_nc};
@@ -1244,7 +1256,7 @@ struct ViscArgs {
   int dt_slot;
   OpacParams op;
 };
-__global__ void __launch_bounds__(128, KC_RIJVISC_MIN_BLOCKS) k_rijvisc(DevState s, ViscArgs a) {
+__global__ void __launch_bounds__(128, KC_RIJVISC_MIN_BLOCKS) k_rijvisc(DevState s, const __grid_constant__ ViscArgs a) {
   const double dt = s.coef[a.dt_slot];
   long xl = s.gr.nx > 1, yl = s.gr.ny > 1, zl = s.gr.nz > 1;
   Range r = {-xl, -yl, -zl, s.gr.nx + 2 * xl, s.gr.ny + 2 * yl, s.gr.nz + 2 * zl};

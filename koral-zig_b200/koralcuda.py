@@ -23,6 +23,7 @@ KC_ERR_INVALID_CONFIG = 1
 KC_ERR_OOM = 2
 KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
+KC_FP32_PPM, KC_FP32_LAXF, KC_FP32_CT, KC_FP32_FLUX = 2, 4, 8, 16
 KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT, KC_IMPLICIT_SORTED = 0, 1, 2, 3
 KC_NPASS = 14
 KC_ERR_TOO_MANY_CELLS = 9
@@ -90,7 +91,8 @@ class KcDumpHeader(ctypes.Structure):
 class KcTuneResult(ctypes.Structure):
     _fields_ = [("implicit_mode", ctypes.c_int32), ("tpb_implicit", ctypes.c_int32), ("tpb_flux", ctypes.c_int32),
                 ("tpb_u2p", ctypes.c_int32), ("ms_per_step", _d), ("ms_per_step_entry", _d),
-                ("trials", ctypes.c_int32), ("implicit_phi_fastest", ctypes.c_int32)]
+                ("trials", ctypes.c_int32), ("implicit_phi_fastest", ctypes.c_int32),
+                ("implicit_min_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class KcStepInfo(ctypes.Structure):
@@ -166,6 +168,7 @@ def lib():
     L.kc_debug_phase.argtypes = [vp, ctypes.c_int, dbl]
     L.kc_debug_get_array.argtypes = [vp, ctypes.c_int, vp]
     L.kc_debug_fail_allocs.argtypes = [vp, i32]
+    L.kc_flux_ct.argtypes = [i32] * 5 + [vp] * 3
     for n in ["kc_create", "kc_upload_prims", "kc_upload_cons", "kc_download_prims", "kc_download_cons",
               "kc_upload_flags", "kc_download_flags", "kc_set_counters", "kc_get_counters", "kc_finish_init",
               "kc_init_timestep_guess", "kc_set_bc", "kc_calc_u2p", "kc_cfl_dt", "kc_step", "kc_step_n",
@@ -175,7 +178,7 @@ def lib():
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
               "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune",
               "kc_kdmp_write_header", "kc_kdmp_parse_header", "kc_kdmp_write", "kc_kdmp_load", "kc_kdmp_write_file",
-              "kc_kdmp_load_file", "kc_debug_fail_allocs"]:
+              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -428,6 +431,18 @@ def implicit_batch(opt, geom23, dt, pp, mode=KC_IMPLICIT_PER_CELL):
     if st != KC_OK:
         raise KoralError(st, "kc_implicit_batch")
     return pp, res
+
+
+def flux_ct(nx, ny, nz, ng, fb, device=0):
+    """ct.fluxCt (koral/sim/ct.zig:38) on face-flux B rows: fb is a list of
+    three arrays (None for an inactive direction) in the FaceStore layout,
+    shape (FZ, FY, FX, 3); returns rebuilt copies."""
+    out = [None if f is None else np.ascontiguousarray(f, dtype=np.float64).copy() for f in fb]
+    ptr = [None if f is None else f.ctypes.data for f in out]
+    st = lib().kc_flux_ct(device, nx, ny, nz, ng, *ptr)
+    if st != KC_OK:
+        raise KoralError(st, "kc_flux_ct")
+    return out
 
 
 def implicit_batch_noalloc(opt, geom23, dt, pp, mode=KC_IMPLICIT_PER_CELL):

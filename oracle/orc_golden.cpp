@@ -251,7 +251,7 @@ extern "C" int orc_golden(const char* name, long nrec, const double* in, int nin
       fill_rad_state(pp00, g, kGam, op, true, st00);
       p2u(cand, uux, g, kGam);
       fill_rad_state(cand, g, kGam, op, true, stx);
-      o[0] = implicit_residual(uux, cand, stx, uu00, st00, dt, g, op, (int)a[50], (int)a[51], (int)a[52], f);
+      o[0] = implicit_residual(uux, cand, stx, uu00, st00, dt, g, op, op.opdamp, (int)a[50], (int)a[51], (int)a[52], f);
     } else if (!strcmp(name, "metric_points")) {
       // coords, x0..x3 -> gg16 GG16 gdet dlgdet3 Kr64 gttpert
       int id = (int)a[0];

@@ -278,3 +278,53 @@ def test_production_2d_grid_ten_steps_bitwise():
     cg, co = gpu.counters(), orc.counters()
     for k in ["t", "dt", "tstepdenmax", "tstepdenmin", "n_radimp_failures", "n_radimp_iters", "n_radimp_solves"]:
         assert cg[k] == co[k], (k, cg[k], co[k])
+
+
+def _face_shape(nx, ny, nz, ng, dim):
+    sx, sy, sz = (n + 2 * ng if n > 1 else 1 for n in (nx, ny, nz))
+    return (sz + (dim == 2), sy + (dim == 1), sx + (dim == 0))
+
+
+def _oracle_flux_ct(nx, ny, nz, ng, fb):
+    from tests.orcsim import _bind
+
+    out = [None if f is None else f.copy() for f in fb]
+    _bind().orc_flux_ct(nx, ny, nz, ng, *[None if f is None else f.ctypes.data for f in out])
+    return out
+
+
+def test_flux_ct_device_on_golden_records():
+    """kc_flux_ct (the step's flux-CT kernels) on the reference's flux/ct
+    golden records (koral/tests/golden/step_golden_tests.zig:299): bit for
+    bit with the oracle, and within the reference's 1e-15 of C's outputs."""
+    kc = _kc()
+    i, o = load_kgld("flux/ct")
+    nx, ny, nz, ng = 32, 32, 1, 3
+    fb = [np.zeros(_face_shape(nx, ny, nz, ng, d) + (3,)) for d in range(2)] + [None]
+    dims, ix, iy = i[:, 0].astype(int), i[:, 1].astype(int) + ng, i[:, 2].astype(int) + ng
+    for d in range(2):
+        m = dims == d
+        fb[d][0, iy[m], ix[m], :] = i[m, 3:6]
+    g = kc.flux_ct(nx, ny, nz, ng, fb)
+    z = _oracle_flux_ct(nx, ny, nz, ng, fb)
+    for d in range(2):
+        assert np.array_equal(_bits(g[d]), _bits(z[d]))
+    got = np.array([g[d][0, y, x, :] for d, x, y in zip(dims, ix, iy)])
+    assert np.max(np.abs(got - o) / np.maximum(1.0, np.maximum(np.abs(got), np.abs(o)))) <= 1e-15
+
+
+@pytest.mark.parametrize("shape", [(12, 10, 6), (1, 9, 7), (8, 1, 5)])
+def test_flux_ct_device_3d_bitwise(shape):
+    """Random face fluxes on 3D and collapsed-dimension grids (the 0.25 and
+    0.5 EMF coefficients, pinned indices): device == oracle bit for bit."""
+    kc = _kc()
+    nx, ny, nz = shape
+    ng = 3
+    rng = np.random.default_rng(sum(shape))
+    fb = [rng.standard_normal(_face_shape(nx, ny, nz, ng, d) + (3,)) if n > 1 else None
+          for d, n in enumerate(shape)]
+    g = kc.flux_ct(nx, ny, nz, ng, fb)
+    z = _oracle_flux_ct(nx, ny, nz, ng, fb)
+    for d in range(3):
+        if fb[d] is not None:
+            assert np.array_equal(_bits(g[d]), _bits(z[d])), d

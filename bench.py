@@ -229,6 +229,63 @@ def oracle_implicit_rate(geom, dt, pp, threads, min_seconds=10.0):
     return done / t, done, t
 
 
+def implicit_battery(kc, opt, stream, rounds=30):
+    """The reference's own implicit battery (koral tools/bench_implicit.zig:96-221):
+    the 336 rad_implicit golden records (tests/golden, converted from the
+    reference's rad_implicit.kgld), timed in ns/solve as that tool times them,
+    on the GPU (the 336 cells per launch, and the battery replicated to 2^20
+    cells so that it fills the device) and on the oracle port (one host thread,
+    and all host threads with a dynamic ticket)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    z = np.load(os.path.join(ROOT, "tests", "golden", "rad__rad_implicit.npz"))
+    d = np.ascontiguousarray(z["data"])
+    geom, dt, pp = d[:, :23].copy(), d[:, 23].copy(), d[:, 24:37].copy()
+    nrec = len(dt)
+    out = {"records": nrec, "rounds": rounds}
+    for label, reps in (("gpu_battery", 1), ("gpu_battery_x3121", 3121)):
+        g = torch.from_numpy(np.tile(geom, (reps, 1))).cuda()
+        t = torch.from_numpy(np.tile(dt, reps)).cuda()
+        p0 = torch.from_numpy(np.tile(pp, (reps, 1))).cuda()
+        p = torch.empty_like(p0)
+        r = torch.zeros((nrec * reps, 6), dtype=torch.int32, device="cuda")
+
+        def go():
+            p.copy_(p0)
+            kc.implicit_batch_device(opt, nrec * reps, g.data_ptr(), t.data_ptr(), p.data_ptr(), r.data_ptr(),
+                                     stream.cuda_stream, mode=0)
+
+        go()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(rounds):
+            go()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[label + "_ns_per_solve"] = e0.elapsed_time(e1) * 1e6 / (rounds * nrec * reps)
+        if reps == 1:
+            out["converged"] = int((r[:, 0] == 1).sum().item())
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    lib.orc_implicit_batch_mt.argtypes = [ctypes.c_long] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+    threads = os.cpu_count() or 1
+    for label, th in (("oracle_1_thread", 1), (f"oracle_{threads}_threads", threads)):
+        done, el = 0, 0.0
+        while el < 2.0:
+            q = pp.copy()
+            res = np.zeros((nrec, 3), dtype=np.int32)
+            t0 = time.perf_counter()
+            lib.orc_implicit_batch_mt(nrec, geom.ctypes.data, dt.ctypes.data, q.ctypes.data, res.ctypes.data, th)
+            el += time.perf_counter() - t0
+            done += nrec
+        out[label + "_ns_per_solve"] = el * 1e9 / done
+    return out
+
+
 def run_implicit(args, rank, world, local):
     """The batched implicit M1 solve over 2^22 independent seeded cells
     (kc_synth_implicit_cells), inputs resident in HBM, FP64."""
@@ -308,6 +365,7 @@ def run_implicit(args, rank, world, local):
                      "algorithmic_bytes": bpc * n},
         "clocks": clk, "gpu_launches": args.steps,
     }
+    line["reference_battery"] = implicit_battery(kc, opt, stream)
     if rank == 0 and not args.no_cpu_baseline:
         rate, done, t = oracle_implicit_rate(geom[:sample_n], dt[:sample_n], pp[:sample_n], threads)
         line["cpu_baseline"] = {"value": rate, "unit": IMPL_UNIT, "cores": threads, "kind": "port",
@@ -385,9 +443,32 @@ def run_precision(args, rank, local):
         for part in name.split("+"):
             mode |= piece[part]
         variants.append(("mixed" if name == "all" else "mixed_" + name, mode))
-    for form, mode in [("fp64", 0)] + variants + [("fp64_seeded", 0)]:
+    weights = None
+    train = None
+    if args.combined:
+        # the learned guess of the combined form: pairs harvested from a separate
+        # run of the same wedge and init, network trained on the GPU
+        src = kc.Sim(grid, kc.puffy_options(device=local))
+        src.initPuffy(1e-3, 1e-3, args.seed)
+        src.harvest_implicit(args.pairs)
+        hsteps = 0
+        while True:
+            src.step()
+            hsteps += 1
+            x, t = src.get_harvest(args.pairs)
+            if x.shape[0] >= args.pairs or hsteps >= 20:
+                break
+        src.close()
+        weights, loss = kc.mlp_train(x, t, steps=args.train_steps, batch=1024, lr=2e-3, seed=3)
+        train = {"pairs": int(x.shape[0]), "harvest_steps": hsteps, "minibatches": args.train_steps,
+                 "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-100:].mean())}
+        variants = variants + [("combined", kc.KC_MIXED, weights), ("fp64_guess", 0, weights)]
+    variants = [v if len(v) == 3 else (v[0], v[1], None) for v in variants]
+    for form, mode, w in [("fp64", 0, None)] + variants + [("fp64_seeded", 0, None)]:
         sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode))
         sim.initPuffy(1e-3, 1e-3, args.seed)
+        if w is not None:
+            sim.set_guess(w)
         if form == "fp64_seeded":
             # the FP64 run's own sensitivity: a 1e-15 relative seed on the conserved density
             u = sim.u
@@ -405,8 +486,11 @@ def run_precision(args, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        c = sim.counters()
         out[form] = {"p": sim.p, "scalars": sim.scalars(0.0, 5000.0, 15.0), "ms_per_step": ms / args.steps,
-                     "value": args.nx * args.ny * args.nz * args.steps / (ms / 1e3)}
+                     "value": args.nx * args.ny * args.nz * args.steps / (ms / 1e3),
+                     "newton_per_solve": c["n_radimp_iters"] / max(c["n_radimp_solves"], 1),
+                     "implicit_failures": c["n_radimp_failures"]}
         sim.close()
     b = out["fp64"]["p"]
     ok = np.all(np.isfinite(b), axis=1)
@@ -423,9 +507,14 @@ def run_precision(args, rank, local):
             "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms_per_step"]},
             "fp64_seed_1e-15": {"field_scale": dict(zip(names, dev_s.tolist())), "integrated_rel": rel_s},
             "scalars_fp64": out["fp64"]["scalars"]}
-    for form, mode in variants:
+    line["fp64"]["newton_per_solve"] = out["fp64"]["newton_per_solve"]
+    if train is not None:
+        line["guess_training"] = train
+    for form, mode, w in variants:
         dev, rel = dev_of(form)
-        line[form] = {"precision_mode": mode, "value": out[form]["value"], "ms_per_step": out[form]["ms_per_step"],
+        line[form] = {"precision_mode": mode, "learned_guess": w is not None, "value": out[form]["value"],
+                      "ms_per_step": out[form]["ms_per_step"], "newton_per_solve": out[form]["newton_per_solve"],
+                      "implicit_failures": out[form]["implicit_failures"],
                       "field_scale_error": dict(zip(names, dev.tolist())), "integrated_rel_error": rel,
                       "scalars": out[form]["scalars"]}
     if rank == 0:
@@ -541,6 +630,8 @@ def main():
                     help="skip the autotuner (implicit form and block sizes) before the timed steps")
     ap.add_argument("--no-forms", dest="forms", action="store_false",
                     help="skip the mixed-vs-plain comparison of the default workload")
+    ap.add_argument("--combined", action="store_true",
+                    help="precision workload: add the combined form (mixed + learned guess) and FP64 + learned guess")
     ap.add_argument("--mixed-forms", default="all",
                     help="precision workload: comma-separated FP32 piece sets (all, ppm, laxf, ct, flux, "
                          "or a+b combinations) run beside plain FP64")

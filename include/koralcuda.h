@@ -252,22 +252,29 @@ int kc_debug_fail_allocs(kc_handle* h, int32_t n);
  * form (precision, implicit form, guess, harvest) runs eagerly, the next one is
  * captured. Pass timing (kc_set_pass_timing) runs the steps eagerly. */
 int kc_set_graph(kc_handle* h, int32_t on);
+/* The y and z face sweeps' form (no reference counterpart; every form gives the
+ * same bits): 0 one thread per face reconstructing both of its neighbour cells
+ * (the default), 1 blocks of 32 columns x 4 faces that reconstruct each cell
+ * once into shared memory, 2 the same with the PPM stencil rows staged in
+ * shared memory too. kc_autotune picks among them. */
+int kc_set_face_tiles(kc_handle* h, int32_t mode);
 
 /* The autotuner's choice (no reference counterpart): implicit form
  * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT), threads per block of the
  * per-cell implicit, face-flux and u2p kernels, and the per-cell implicit
  * kernel's thread -> cell order (1, the default: phi fastest on 3D grids, so
  * that a warp's cells share r and theta, theta fastest on 2D grids; 0: x
- * fastest) and its register budget (resident blocks of 128 threads per SM: 2
- * with 255 registers per thread, 3 with 168), with the measured step time of
- * the choice and of the configuration on entry. */
+ * fastest), its register budget (resident blocks of 128 threads per SM: 2
+ * with 255 registers per thread, 3 with 168) and whether the y and z face
+ * sweeps stage their PPM stencils in shared-memory tiles, with the measured
+ * step time of the choice and of the configuration on entry. */
 typedef struct kc_tune_result {
   int32_t implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
   double ms_per_step, ms_per_step_entry;
   int32_t trials;
   int32_t implicit_phi_fastest;
   int32_t implicit_min_blocks; /* 2: 255 registers per thread, 3: 168; 0: by cell order */
-  int32_t reserved;
+  int32_t face_tiles;          /* the y and z face sweeps' form (kc_set_face_tiles) */
 } kc_tune_result;
 /* Times whole steps on the handle's current state for each candidate, one
  * knob at a time, and keeps the fastest configuration set; the state and the

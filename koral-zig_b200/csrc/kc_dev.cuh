@@ -80,21 +80,31 @@ KC_HD int sym10(int i, int j) {
   return i == 0 ? j : i == 1 ? 3 + j : i == 2 ? 5 + j : 9;
 }
 
+// A load of data read once per launch; with STREAM it is marked evict-first in
+// L2 (ld.global.cs), so that it does not push out what the kernel reuses.
+template <bool STREAM = false>
+__device__ __forceinline__ double ld_once(const double* p) {
+  if (STREAM) return __ldcs(p);
+  return *p;
+}
+template <bool STREAM = false>
 __device__ __forceinline__ void geom_load(const double* gc, const double* Gc, long stride, long c, double x1, double x2,
                                           double x3, Geom& g) {
+  double sym[10];
+  for (int k = 0; k < 10; ++k) sym[k] = ld_once<STREAM>(gc + (long)k * stride + c);
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) {
-      g.gg[i][j] = gc[(long)sym10(i, j) * stride + c];
-      g.GG[i][j] = Gc[(long)(i * 4 + j) * stride + c];
+      g.gg[i][j] = sym[sym10(i, j)];
+      g.GG[i][j] = ld_once<STREAM>(Gc + (long)(i * 4 + j) * stride + c);
     }
   g.gg[0][4] = 0.0;
   g.gg[1][4] = 0.0;
   g.gg[2][4] = 0.0;
-  g.gg[3][4] = gc[10L * stride + c];
+  g.gg[3][4] = ld_once<STREAM>(gc + 10L * stride + c);
   g.GG[0][4] = 0.0;
   g.GG[1][4] = 0.0;
   g.GG[2][4] = 0.0;
-  g.GG[3][4] = Gc[16L * stride + c];
+  g.GG[3][4] = ld_once<STREAM>(Gc + 16L * stride + c);
   g.xx[0] = 0.0;
   g.xx[1] = x1;
   g.xx[2] = x2;
@@ -111,9 +121,10 @@ __device__ __forceinline__ long face_index(const DGrid& gr, int dim, long ix, lo
   if (dim == 1) return jx + jy * gr.sx + jz * (gr.sy + 1) * gr.sx;
   return jx + jy * gr.sx + jz * gr.sy * gr.sx;
 }
+template <bool STREAM = false>
 __device__ __forceinline__ void geom_cell(const DevState& s, long ix, long iy, long iz, Geom& g) {
-  geom_load(s.cgc, s.cGc, s.gr.nc, cidx(s.gr, ix, iy, iz), grid_xc(s.gr.g, ix), grid_yc(s.gr.g, iy),
-            grid_zc(s.gr.g, iz), g);
+  geom_load<STREAM>(s.cgc, s.cGc, s.gr.nc, cidx(s.gr, ix, iy, iz), grid_xc(s.gr.g, ix), grid_yc(s.gr.g, iy),
+                    grid_zc(s.gr.g, iz), g);
 }
 __device__ __forceinline__ void geom_face(const DevState& s, long ix, long iy, long iz, int dim, Geom& g) {
   double x1 = dim == 0 ? grid_xl(s.gr.g, ix) : grid_xc(s.gr.g, ix);
@@ -141,13 +152,18 @@ __device__ __forceinline__ void geom_bl(const DevState& s, long c, Geom& g) {
   g.gttpert = 0.0;
   g.alpha = kmath::sqrt(-1.0 / g.GG[0][0]);
 }
+template <bool STREAM = false>
 __device__ __forceinline__ void load_cell(const double* f, long nc, long c, double v[NV]) {
 #pragma unroll
-  for (int i = 0; i < NV; ++i) v[i] = f[i * nc + c];
+  for (int i = 0; i < NV; ++i) v[i] = ld_once<STREAM>(f + i * nc + c);
 }
+template <bool STREAM = false>
 __device__ __forceinline__ void store_cell(double* f, long nc, long c, const double v[NV]) {
 #pragma unroll
-  for (int i = 0; i < NV; ++i) f[i * nc + c] = v[i];
+  for (int i = 0; i < NV; ++i) {
+    if (STREAM) __stcs(f + i * nc + c, v[i]);
+    else f[i * nc + c] = v[i];
+  }
 }
 __device__ __forceinline__ void kr_block(const DevState& s, long c, double k[64]) {
   for (int l = 0; l < 4; ++l)

@@ -79,6 +79,10 @@ struct kc_handle {
   // resident blocks of 128 per SM the per-cell implicit kernel's registers allow:
   // 2 (255 registers) or 3 (168); 0 picks by cell order (2 when phi is fastest)
   int implicit_min_blocks = 0;
+  // the y and z face sweeps of the plain form: 0 one thread per face with its own
+  // two PPMs, 1 tiles with the reconstructed faces in shared memory, 2 tiles that
+  // also stage the stencil rows in shared memory
+  int face_tiles = 0;
   // the step's dt-derived coefficients: pinned host table and its device copy
   // (DevState::coef); slots 0-3 are fixed by run_step, later ones appended
   double* coef_host = nullptr;
@@ -502,6 +506,17 @@ void launch_face_fluxes(kc_handle* h) {
     if (dim == 0) {
       if (mx) k_face_flux<true, 0><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
       else k_face_flux<false, 0><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
+    } else if (!mx && h->face_tiles) {
+      // FT_COLS transverse columns x FT_FACES faces per block of 4 warps
+      dim3 grid((unsigned)((n0 * n1 + FT_COLS - 1) / FT_COLS), (unsigned)((dims[dim] + 1 + FT_FACES - 1) / FT_FACES));
+      const unsigned tb4 = 32 * FT_FACES;
+      if (h->face_tiles == 2) {  // stencil rows staged in shared memory
+        if (dim == 1) k_face_flux_tiled<1, true><<<grid, tb4, sizeof(FaceTile), h->stream>>>(h->ds, h->dsc, a);
+        else k_face_flux_tiled<2, true><<<grid, tb4, sizeof(FaceTile), h->stream>>>(h->ds, h->dsc, a);
+      } else {  // stencil through L1, reconstructed faces in shared memory
+        if (dim == 1) k_face_flux_tiled<1, false><<<grid, tb4, sizeof(FaceTileOut), h->stream>>>(h->ds, h->dsc, a);
+        else k_face_flux_tiled<2, false><<<grid, tb4, sizeof(FaceTileOut), h->stream>>>(h->ds, h->dsc, a);
+      }
     } else if (dim == 1) {
       if (mx) k_face_flux<true, 1><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
       else k_face_flux<false, 1><<<nb, tb, 0, h->stream>>>(h->ds, h->dsc, a);
@@ -862,6 +877,12 @@ int kc_create(const kc_grid* grid, const kc_options* opt, kc_handle** out) {
   int st = cuda_check(h, cudaSetDevice(opt->device), "cudaSetDevice");
   if (st) return st;
   st = cuda_check(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (st) return st;
+  // the tiled face kernels stage more than the default 48 KB of shared memory
+  st = cuda_check(h, cudaFuncSetAttribute(k_face_flux_tiled<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(FaceTile)), "face tile shared memory");
+  if (!st) st = cuda_check(h, cudaFuncSetAttribute(k_face_flux_tiled<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)sizeof(FaceTile)), "face tile shared memory");
   if (st) return st;
   Grid g = grid_init(grid->nx, grid->ny, grid->nz, grid->ng, grid->minx, grid->maxx, grid->miny, grid->maxy, grid->minz,
                      grid->maxz);
@@ -1287,6 +1308,16 @@ static int ensure_imp_ctr(kc_handle* h) {
 }
 // The CUDA graph form of the step (no reference counterpart): on, the whole
 // step's launch sequence is captured once and replayed (bit-identical).
+// The y and z face sweeps' form (no reference counterpart; all bit-identical):
+// 0 one thread per face, 1 shared-memory tiles of reconstructed faces, 2 tiles
+// that also stage the stencil rows.
+int kc_set_face_tiles(kc_handle* h, int32_t mode) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (mode < 0 || mode > 2) return reject(h, KC_ERR_INVALID_CONFIG, "unknown face-tile mode");
+  h->face_tiles = mode;
+  drop_graph(h);
+  return KC_OK;
+}
 int kc_set_graph(kc_handle* h, int32_t on) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   if (h->stream) cudaStreamSynchronize(h->stream);

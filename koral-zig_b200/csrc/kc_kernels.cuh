@@ -909,6 +909,120 @@ __global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux(DevState 
                                                          : laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
 }
 
+// ---- face fluxes through shared-memory tiles (sweeps along y and z) ---------------
+// The same face fluxes as k_face_flux<false, DIM>, bit for bit, with the PPM
+// stencils staged in shared memory. A block takes FT_COLS transverse columns
+// (x fastest, then the other transverse index, linearised so that no lane
+// idles at the end of an x row) and FT_FACES consecutive faces along the sweep.
+// It loads the FT_FACES + 5 cells of each column that the faces' stencils
+// cover, 13 variables, with coalesced loads; reconstructs each of the
+// FT_FACES + 1 cells the faces need once (one PPM gives a cell's left and right
+// face values, against two PPMs per face when each face reconstructs both of
+// its neighbours); and then each thread forms one face's two states, one-sided
+// fluxes and LAXF flux from the staged values.
+constexpr int FT_COLS = 32, FT_FACES = 4, FT_ROWS = FT_FACES + 5, FT_REC = FT_FACES + 1, FT_LW = FT_COLS + 1;
+// STAGE = false keeps the stencil reads in L1 and stages only the reconstructed
+// face values (27 KB of shared memory per block instead of 59 KB, more L1 for
+// the kernel's metric loads and call frames).
+struct FaceTileOut {
+  double fr[FT_FACES][NV][FT_LW];   // right value of cell f-1: the left state of face f
+  double fl[FT_FACES][NV][FT_LW];   // left value of cell f: the right state of face f
+  PpmCoef coef[FT_REC];             // width factors of cells f0-1 .. f0+FT_FACES-1
+};
+struct FaceTile {
+  FaceTileOut o;
+  double p[NV][FT_ROWS][FT_LW];     // stencil rows f0-3 .. f0+FT_FACES+1
+};
+template <int DIM, bool STAGE>
+__global__ void __launch_bounds__(128, KC_FLUX_MIN_BLOCKS) k_face_flux_tiled(DevState s, DevScalars* sc,
+                                                                               const __grid_constant__ FluxArgs a) {
+  static_assert(DIM == 1 || DIM == 2, "tiles are along y or z");
+  extern __shared__ __align__(16) unsigned char ft_smem[];
+  FaceTile& T = *reinterpret_cast<FaceTile*>(ft_smem);  // only T.o exists when !STAGE
+  constexpr int dim = DIM, c0d = 0, c1d = DIM == 1 ? 2 : 1;
+  const long n = dim == 1 ? s.gr.ny : s.gr.nz;
+  const long dims[3] = {s.gr.nx, s.gr.ny, s.gr.nz};
+  const long lo0 = dims[c0d] > 1 ? -1 : 0, n0 = dims[c0d] > 1 ? dims[c0d] + 2 : dims[c0d];
+  const long lo1 = dims[c1d] > 1 ? -1 : 0, n1 = dims[c1d] > 1 ? dims[c1d] + 2 : dims[c1d];
+  const long ncols = n0 * n1, col0 = (long)blockIdx.x * FT_COLS, f0 = (long)blockIdx.y * FT_FACES;
+  const long ng = dim == 1 ? s.gr.ngy : s.gr.ngz;
+  const int tid = threadIdx.x;
+  const Grid& g = s.gr.g;
+  const long nc = s.gr.nc;
+  // global index of the stencil cell of column col at sweep index sw (-1: outside the stored grid)
+  auto stencil_cell = [&](long col, long sw) -> long {
+    if (col >= ncols || sw < -ng || sw >= n + ng) return -1;
+    long cc[3];
+    cc[c0d] = lo0 + col % n0;
+    cc[c1d] = lo1 + col / n0;
+    cc[dim] = sw;
+    return cidx(s.gr, cc[0], cc[1], cc[2]);
+  };
+  // 1. stage the stencil rows of the block's columns (rows outside the stored grid stay unread)
+  for (int k = tid; STAGE && k < NV * FT_ROWS * FT_COLS; k += blockDim.x) {
+    const int l = k % FT_COLS, q = k / FT_COLS, r = q % FT_ROWS, iv = q / FT_ROWS;
+    const long cj = stencil_cell(col0 + l, f0 - 3 + r);
+    T.p[iv][r][l] = cj >= 0 ? s.p[(long)iv * nc + cj] : 0.0;
+  }
+  if (tid < FT_REC) {
+    double dxs[5];
+    for (int k = 0; k < 5; ++k) dxs[k] = cell_size(g, f0 - 3 + tid + k, dim);
+    T.o.coef[tid] = ppm_coef(dxs);
+  }
+  __syncthreads();
+  // 2. one PPM per (cell, variable, column)
+  for (int k = tid; k < NV * FT_REC * FT_COLS; k += blockDim.x) {
+    const int l = k % FT_COLS, q = k / FT_COLS, rc = q % FT_REC, iv = q / FT_REC;
+    double u[5];
+    if (STAGE) {
+      for (int j = 0; j < 5; ++j) u[j] = T.p[iv][rc + j][l];
+    } else {
+      for (int j = 0; j < 5; ++j) {
+        const long cj = stencil_cell(col0 + l, f0 - 3 + rc + j);
+        u[j] = cj >= 0 ? s.p[(long)iv * nc + cj] : 0.0;
+      }
+    }
+    const Faces fc = ppm_apply(u, T.o.coef[rc]);
+    if (rc < FT_FACES) T.o.fr[rc][iv][l] = fc.right;
+    if (rc > 0) T.o.fl[rc - 1][iv][l] = fc.left;
+  }
+  __syncthreads();
+  // 3. one face per thread
+  const int w = tid >> 5, lane = tid & 31;
+  const long f = f0 + w, col = col0 + lane;
+  if (f > n || col >= ncols) return;
+  long cf[3];
+  cf[dim] = f;
+  cf[c0d] = lo0 + col % n0;
+  cf[c1d] = lo1 + col / n0;
+  double pL[NV], pR[NV];
+  for (int iv = 0; iv < NV; ++iv) {
+    pL[iv] = T.o.fr[w][iv][lane];
+    pR[iv] = T.o.fl[w][iv][lane];
+  }
+  long cc[3] = {cf[0], cf[1], cf[2]};
+  cc[dim] = f;
+  const long c = cidx(s.gr, cc[0], cc[1], cc[2]);
+  cc[dim] = f - 1;
+  const long cm = cidx(s.gr, cc[0], cc[1], cc[2]);
+  Geom geo;
+  geom_face(s, cf[0], cf[1], cf[2], dim, geo);
+  double ffl[NV], ffr[NV], uL[NV], uR[NV];
+  int e = face_state(s, sc, a, dim, pL, geo, c, cm, ffl, uL);
+  if (!e) e = face_state(s, sc, a, dim, pR, geo, c, cm, ffr, uR);
+  if (e) {
+    set_err(sc, e, c);
+    return;
+  }
+  const double ag = kmath::fmax(s.amax[(long)dim * nc + c], s.amax[(long)dim * nc + cm]);
+  const double agr = kmath::fmax(s.amax[(long)(3 + dim) * nc + c], s.amax[(long)(3 + dim) * nc + cm]);
+  const long fi = face_index(s.gr, dim, cf[0], cf[1], cf[2]);
+  double* out = s.flb[dim];
+  const long nfd = s.nf[dim];
+#pragma unroll
+  for (int iv = 0; iv < NV; ++iv) out[iv * nfd + fi] = laxf(ffl[iv], ffr[iv], uL[iv], uR[iv], iv >= EE ? agr : ag);
+}
+
 // ---- flux-CT (koral/sim/ct.zig:38) --------------------------------------------
 __device__ __forceinline__ long pin(long n, long i) { return n == 1 ? 0 : i; }
 __device__ __forceinline__ double flbv(const DevState& s, int dim, int iv, long ix, long iy, long iz) {
@@ -1068,11 +1182,14 @@ __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* 
   }
   if (a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) return;
   long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  // the cell's metric is read once and its state written once: evict-first in
+  // L2 (which keeps L2 for the solver's call frames); the state loads stay plain
+  // (their evict-first form costs the kernel registers and 200 bytes of spills)
   double uu[NV], pp[NV];
   load_cell(s.u, nc, c, uu);
   load_cell(s.p, nc, c, pp);
   Geom g;
-  geom_cell(s, ix, iy, iz, g);
+  geom_cell<true>(s, ix, iy, iz, g);
   double pp00[NV];
   if (EXTRA)
     for (int i = 0; i < NV; ++i) pp00[i] = pp[i];
@@ -1099,8 +1216,8 @@ __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* 
     }
   }
   if (res.ok) {
-    store_cell(s.u, nc, c, uu);
-    store_cell(s.p, nc, c, pp);
+    store_cell<true>(s.u, nc, c, uu);
+    store_cell<true>(s.p, nc, c, pp);
     s.flags[5 * nc + c] = 0;
     atomicAdd(&sc->n_iters, (unsigned long long)res.iters);
     atomicAdd(&sc->n_solves, 1ULL);

@@ -92,7 +92,7 @@ class KcTuneResult(ctypes.Structure):
     _fields_ = [("implicit_mode", ctypes.c_int32), ("tpb_implicit", ctypes.c_int32), ("tpb_flux", ctypes.c_int32),
                 ("tpb_u2p", ctypes.c_int32), ("ms_per_step", _d), ("ms_per_step_entry", _d),
                 ("trials", ctypes.c_int32), ("implicit_phi_fastest", ctypes.c_int32),
-                ("implicit_min_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("implicit_min_blocks", ctypes.c_int32), ("face_tiles", ctypes.c_int32)]
 
 
 class KcStepInfo(ctypes.Structure):
@@ -134,6 +134,7 @@ def lib():
     L.kc_set_precision.argtypes = [vp, i32]
     L.kc_set_implicit_mode.argtypes = [vp, i32]
     L.kc_set_graph.argtypes = [vp, i32]
+    L.kc_set_face_tiles.argtypes = [vp, i32]
     L.kc_autotune.argtypes = [vp, i32, P(KcTuneResult)]
     L.kc_set_guess.argtypes = [vp, i32, vp, i64]
     L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64, P(dbl)]
@@ -178,7 +179,7 @@ def lib():
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
               "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune",
               "kc_kdmp_write_header", "kc_kdmp_parse_header", "kc_kdmp_write", "kc_kdmp_load", "kc_kdmp_write_file",
-              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct"]:
+              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct", "kc_set_face_tiles"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -310,6 +311,11 @@ class Sim:
     def set_graph(self, on):
         """Capture the step as a CUDA graph and replay it (bit-identical)."""
         self._check(self._lib.kc_set_graph(self._h, 1 if on else 0))
+
+    def set_face_tiles(self, mode):
+        """The y and z face sweeps' form: 0 per face, 1 reconstructed-face tiles,
+        2 stencil and reconstructed-face tiles (all bit-identical)."""
+        self._check(self._lib.kc_set_face_tiles(self._h, mode))
 
     def autotune(self, steps=2):
         """kc_autotune: pick the implicit form and block sizes by timing steps on

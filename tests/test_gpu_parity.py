@@ -328,3 +328,21 @@ def test_flux_ct_device_3d_bitwise(shape):
     for d in range(3):
         if fb[d] is not None:
             assert np.array_equal(_bits(g[d]), _bits(z[d])), d
+
+
+@pytest.mark.parametrize("tiles", [1, 2])
+def test_face_tile_forms_bitwise(tiles):
+    """The y and z face sweeps through shared-memory tiles (reconstructed faces;
+    and the PPM stencil rows as well): the perturbed 3D wedge and CFL steps,
+    bit for bit with the oracle, and a 2D grid (y sweep only)."""
+    kc = _kc()
+    for nx, ny, nz in ((24, 20, 8), (32, 30, 1)):
+        grid, opt = kc.puffy_grid(nx, ny, nz), kc.puffy_options()
+        gpu, orc = _pair(grid, opt)
+        gpu.set_face_tiles(tiles)
+        assert gpu.initPuffy(1e-3, 1e-3, 77) == orc.init_puffy(1e-3, 1e-3, 77)
+        orc.lib.orc_sim_init_timestep_guess(orc.h)
+        for _ in range(3):
+            gpu.step()
+            orc.step()
+        _assert_same_state(gpu, orc)

@@ -202,7 +202,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2, "sorted": 3}
+IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2, "sorted": 3, "rungs": 4}
 IMPL_METRIC = "implicit M1 solves/s (batched, independent cells)"
 IMPL_UNIT = "solves/s"
 
@@ -247,6 +247,7 @@ def implicit_battery(kc, opt, stream, rounds=30):
     nrec = len(dt)
     out = {"records": nrec, "rounds": rounds}
     for label, reps in (("gpu_battery", 1), ("gpu_battery_x3121", 3121)):
+        nround = rounds if reps == 1 else 3  # the replicated battery fills the device: 3 launches suffice
         g = torch.from_numpy(np.tile(geom, (reps, 1))).cuda()
         t = torch.from_numpy(np.tile(dt, reps)).cuda()
         p0 = torch.from_numpy(np.tile(pp, (reps, 1))).cuda()
@@ -262,11 +263,11 @@ def implicit_battery(kc, opt, stream, rounds=30):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(rounds):
+        for _ in range(nround):
             go()
         e1.record(stream)
         torch.cuda.synchronize()
-        out[label + "_ns_per_solve"] = e0.elapsed_time(e1) * 1e6 / (rounds * nrec * reps)
+        out[label + "_ns_per_solve"] = e0.elapsed_time(e1) * 1e6 / (nround * nrec * reps)
         if reps == 1:
             out["converged"] = int((r[:, 0] == 1).sum().item())
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
@@ -389,9 +390,20 @@ def measure_forms(kc, grid, local, steps, seed, graph):
     import torch
 
     res, dts = {}, []
-    for form, mode in (("fp64", kc.KC_PLAIN_FP64), ("mixed", kc.KC_MIXED)):
+    # the learned guess of the combined form: pairs from one step of the same wedge
+    src = kc.Sim(grid, kc.puffy_options(device=local))
+    src.initPuffy(1e-3, 1e-3, seed)
+    src.harvest_implicit(1000000)
+    src.step()
+    x, t = src.get_harvest(1000000)
+    src.close()
+    weights, _ = kc.mlp_train(x, t, steps=3000, batch=1024, lr=2e-3, seed=3)
+    for form, mode, w in (("fp64", kc.KC_PLAIN_FP64, None), ("mixed", kc.KC_MIXED, None),
+                          ("combined", kc.KC_MIXED, weights)):
         sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode))
         sim.initPuffy(1e-3, 1e-3, seed)
+        if w is not None:
+            sim.set_guess(w)
         sim.set_graph(graph)
         stream = torch.cuda.ExternalStream(sim.stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -407,17 +419,21 @@ def measure_forms(kc, grid, local, steps, seed, graph):
         res[form] = {"ms": e0.elapsed_time(e1) / steps, "p": sim.p, "scalars": sim.scalars(0.0, 5000.0, 15.0),
                      "t": sim.counters()["t"]}
         sim.close()
-    b, a = res["fp64"]["p"], res["mixed"]["p"]
+    b = res["fp64"]["p"]
     ok = np.all(np.isfinite(b), axis=1)
-    dev = np.abs(a[ok] - b[ok]).max(axis=0) / np.maximum(np.abs(b[ok]).max(axis=0), 1e-300)
-    rel = {k: abs(res["mixed"]["scalars"][k] / res["fp64"]["scalars"][k] - 1) for k in INTEGRATED}
-    return {"steps": steps, "t": res["fp64"]["t"],
-            "plain_fp64_ms_per_step": res["fp64"]["ms"], "mixed_ms_per_step": res["mixed"]["ms"],
-            "mixed_speedup": res["fp64"]["ms"] / res["mixed"]["ms"],
-            "mixed_field_scale_error": dict(zip(PRIM_NAMES, dev.tolist())),
-            "mixed_integrated_rel_error": rel,
-            "note": "mixed = FP32 PPM on stencil deviations, FP32 LAXF dissipation, FP32 flux-CT; "
-                    "the rest FP64; same init and dt sequence as the plain run"}
+    out = {"steps": steps, "t": res["fp64"]["t"], "plain_fp64_ms_per_step": res["fp64"]["ms"]}
+    for form in ("mixed", "combined"):
+        a = res[form]["p"]
+        dev = np.abs(a[ok] - b[ok]).max(axis=0) / np.maximum(np.abs(b[ok]).max(axis=0), 1e-300)
+        out[form + "_ms_per_step"] = res[form]["ms"]
+        out[form + "_speedup"] = res["fp64"]["ms"] / res[form]["ms"]
+        out[form + "_field_scale_error"] = dict(zip(PRIM_NAMES, dev.tolist()))
+        out[form + "_integrated_rel_error"] = {
+            k: abs(res[form]["scalars"][k] / res["fp64"]["scalars"][k] - 1) for k in INTEGRATED}
+    return {**out,
+            "note": "mixed = FP32 LAXF dissipation and FP32 flux-CT corner averages, the rest FP64; "
+                    "combined = mixed + the learned initial guess (network trained on the GPU on pairs "
+                    "harvested from one step of the same wedge); same init and dt sequence as the plain run"}
 
 
 def run_precision(args, rank, local):
@@ -462,10 +478,11 @@ def run_precision(args, rank, local):
         weights, loss = kc.mlp_train(x, t, steps=args.train_steps, batch=1024, lr=2e-3, seed=3)
         train = {"pairs": int(x.shape[0]), "harvest_steps": hsteps, "minibatches": args.train_steps,
                  "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-100:].mean())}
-        variants = variants + [("combined", kc.KC_MIXED, weights), ("fp64_guess", 0, weights)]
-    variants = [v if len(v) == 3 else (v[0], v[1], None) for v in variants]
-    for form, mode, w in [("fp64", 0, None)] + variants + [("fp64_seeded", 0, None)]:
-        sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode))
+        variants = variants + [("combined", kc.KC_MIXED, weights), ("fp64_guess", 0, weights),
+                               ("fp64_nobisect", 0, None, {"radimp_start_with_bisect": 0})]
+    variants = [tuple(v) + (None,) * (4 - len(v)) for v in variants]
+    for form, mode, w, o in [("fp64", 0, None, None)] + variants + [("fp64_seeded", 0, None, None)]:
+        sim = kc.Sim(grid, kc.puffy_options(device=local, precision=mode, **(o or {})))
         sim.initPuffy(1e-3, 1e-3, args.seed)
         if w is not None:
             sim.set_guess(w)
@@ -510,7 +527,7 @@ def run_precision(args, rank, local):
     line["fp64"]["newton_per_solve"] = out["fp64"]["newton_per_solve"]
     if train is not None:
         line["guess_training"] = train
-    for form, mode, w in variants:
+    for form, mode, w, _ in variants:
         dev, rel = dev_of(form)
         line[form] = {"precision_mode": mode, "learned_guess": w is not None, "value": out[form]["value"],
                       "ms_per_step": out[form]["ms_per_step"], "newton_per_solve": out[form]["newton_per_solve"],
@@ -536,6 +553,7 @@ def run_guess(args, rank, local):
     kc = load_engine()
     src = kc.Sim(kc.puffy_grid(192, 180, 64), kc.puffy_options(device=local))
     src.initPuffy(1e-3, 1e-3, args.seed)
+    src.set_harvest_filter(1 if args.harvest == "hard" else 0)
     src.harvest_implicit(args.pairs)
     hsteps = 0
     while True:
@@ -601,6 +619,7 @@ def run_guess(args, rank, local):
     line = {"metric": METRIC, "unit": UNIT, "workload": f"PUFFY 3D wedge {args.nx}x{args.ny}x{args.nz}, learned guess",
             "steps": args.steps, "warmup": args.warmup, "dtype": "f64 solve, bf16 network",
             "training": {"pairs": int(x.shape[0]), "harvest_steps": hsteps, "source": "PUFFY 3D wedge 192x180x64",
+                         "harvest": args.harvest,
                          "train_steps": args.train_steps, "batch": 1024, "seconds": train_s,
                          "loss_first10": float(loss[:10].mean()), "loss_last100": float(loss[-100:].mean())},
             **out}
@@ -636,9 +655,11 @@ def main():
                     help="precision workload: comma-separated FP32 piece sets (all, ppm, laxf, ct, flux, "
                          "or a+b combinations) run beside plain FP64")
     ap.add_argument("--pairs", type=int, default=1000000, help="training pairs of the guess workload")
+    ap.add_argument("--harvest", default="all", choices=["hard", "all"],
+                    help="guess workload: train on the solves whose pre-solve state must iterate (hard) or on all")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
-    ap.add_argument("--implicit-mode", default=None, choices=["per-cell", "compacting", "split", "sorted"],
+    ap.add_argument("--implicit-mode", default=None, choices=["per-cell", "compacting", "split", "sorted", "rungs"],
                     help="implicit solve form: one thread per cell, the persistent lane-refilling state machine, the "
                          "split opening + compacted-ladder pair, or (batch workload only) the per-cell kernel over "
                          "key-sorted cells; default: sorted for --workload implicit, per-cell otherwise")

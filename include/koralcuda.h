@@ -55,7 +55,9 @@ enum { KC_PLAIN_FP64 = 0, KC_MIXED = 1 };
  * stencil deviations, the LAXF dissipation product, the flux-CT corner
  * averages, and the one-sided face fluxes rounded to FP32 (their arithmetic
  * stays FP64: the rounding alone bounds what FP32 flux arithmetic would do).
- * KC_MIXED is KC_FP32_PPM | KC_FP32_LAXF | KC_FP32_CT. */
+ * KC_MIXED is KC_FP32_LAXF | KC_FP32_CT: the pieces that keep the integrated
+ * accretion rate and luminosity within 1e-4 of plain FP64 after 1000 steps of
+ * the 192x180x64 wedge (the FP32 reconstruction alone moves them by 9e-3). */
 enum { KC_FP32_PPM = 2, KC_FP32_LAXF = 4, KC_FP32_CT = 8, KC_FP32_FLUX = 16 };
 enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
 /* implicit pass forms (no reference counterpart; all bit-identical to the
@@ -64,8 +66,17 @@ enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
  * machine; SPLIT an opening kernel that finishes every cell passing the Newton
  * core's first residual test at its warm start and a ladder kernel over the
  * compacted rest; SORTED (the batch entry points only) the per-cell kernel over
- * the cells sorted by start fluid, optical depth and temperature */
-enum { KC_IMPLICIT_PER_CELL = 0, KC_IMPLICIT_COMPACTING = 1, KC_IMPLICIT_SPLIT = 2, KC_IMPLICIT_SORTED = 3 };
+ * the cells sorted by start fluid, optical depth and temperature; RUNGS (the
+ * batch entry points only) the sorted cells prepared once (warm start and
+ * reference state), then one launch per rung of the ladder over the cells the
+ * earlier rungs left unsolved, compacted between rungs */
+enum {
+  KC_IMPLICIT_PER_CELL = 0,
+  KC_IMPLICIT_COMPACTING = 1,
+  KC_IMPLICIT_SPLIT = 2,
+  KC_IMPLICIT_SORTED = 3,
+  KC_IMPLICIT_RUNGS = 4
+};
 
 /* Pass ids of the per-pass timers, the members of koral/sim/timers.zig:4
  * Pass that the device step has. KC_PASS_FLUXES covers the reference's
@@ -308,6 +319,11 @@ int kc_set_guess(kc_handle* h, int32_t mode, const float* weights, int64_t nweig
  * targets, up to `capacity` pairs (0 stops the harvest); kc_get_harvest copies
  * the pairs collected so far out and sets *n. */
 int kc_harvest_implicit(kc_handle* h, int64_t capacity);
+/* Which solves the harvest records: 0 (default) every cell whose solve
+ * converged on the first rung; 1 only those whose pre-solve state fails the
+ * Newton core's first residual test, i.e. the cells a start from the pre-solve
+ * state (the reference's radimp_start_with_bisect = 0) would iterate. */
+int kc_set_harvest_filter(kc_handle* h, int32_t mode);
 int kc_get_harvest(kc_handle* h, float* features, float* targets, int64_t capacity, int64_t* n);
 /* seeded ladders that failed and fell back to the plain solve, since the
  * guess was first installed */

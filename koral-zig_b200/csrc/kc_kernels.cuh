@@ -1152,15 +1152,33 @@ struct ImplExtra {
   unsigned long long* hcount;
   long hcap;
   unsigned long long* n_fallback;  // seeded ladders that failed and fell back to the plain path
+  int hfilter;                     // harvest only cells whose pre-solve state must iterate
 };
-// EXTRA = false is the reference path alone (the guess and harvest code is not
-// compiled into it, so its registers and code size are those of the plain solve)
+// Whether the no-bisection start (the cell's pre-solve state) would have to
+// iterate: its first-rung residual against the Newton core's first exit
+// (conv), as solve_implicit_lab_from evaluates it. Out of line, so that its
+// locals do not enlarge the solve's call frame.
+__device__ __noinline__ bool presolve_needs_newton(const double pp00[NV], const Geom& g, double dt, const ImplArgs& a) {
+  double uu00[NV], pc[NV];
+  p2u(pp00, uu00, g, a.gam);
+  RadState st00;
+  fill_rad_state(pp00, g, a.gam, a.op, true, st00);
+  const double ehat = -calc_ff_rtt(pp00, g, nullptr);
+  const int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
+  const double e0 = implicit_start_residual(uu00, st00, pp00, g, dt, a.gam, a.rp, a.op, 1.0, a.ip, sw, pc);
+  return !(e0 < a.ip.conv);
+}
+// FORM: IMPL_PLAIN is the reference path alone (the guess and harvest code is
+// not compiled into it, so its registers and code size are those of the plain
+// solve); IMPL_GUESS adds the learned start only; IMPL_FULL the learned start
+// and the training-pair harvest.
 // MINB: resident blocks of 128 per SM that the register budget must allow.
 // With the x-fastest cell order (2D grids) 3 (168 registers, 12 warps per SM)
 // measured 2-3% faster than 255 registers (8 warps); with the phi-fastest order
 // of 3D grids, whose warps walk the solver together, 255 registers measured 6%
 // faster than 168 and 128 slower still. The host picks the instance by order.
-template <bool EXTRA, int MINB>
+enum : int { IMPL_PLAIN = 0, IMPL_GUESS = 1, IMPL_FULL = 2 };
+template <int FORM, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
                                                             ImplExtra x) {
   const double dt = s.coef[a.dt_slot];
@@ -1191,10 +1209,11 @@ __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* 
   Geom g;
   geom_cell<true>(s, ix, iy, iz, g);
   double pp00[NV];
-  if (EXTRA)
+  constexpr bool HARVEST = FORM == IMPL_FULL;
+  if (HARVEST)
     for (int i = 0; i < NV; ++i) pp00[i] = pp[i];
   ImplicitResult res;
-  if (EXTRA && x.guess) {
+  if (FORM != IMPL_PLAIN && x.guess) {
     long nd = (long)s.gr.nx * s.gr.ny * s.gr.nz, td = ix + s.gr.nx * (iy + s.gr.ny * iz);
     double g0[NV];
     for (int i = 0; i < NV; ++i) g0[i] = x.guess[i * nd + td];
@@ -1206,7 +1225,7 @@ __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* 
   } else {
     res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
   }
-  if (EXTRA && x.hx && res.ok && res.rung == 0) {
+  if (HARVEST && x.hx && res.ok && res.rung == 0 && (!x.hfilter || presolve_needs_newton(pp00, g, dt, a))) {
     unsigned long long k = atomicAdd(x.hcount, 1ULL);
     if ((long)k < x.hcap) {
       double ehat = -calc_ff_rtt(pp00, g, nullptr);

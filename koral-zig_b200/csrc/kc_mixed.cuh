@@ -1,7 +1,9 @@
 // kc_mixed.cuh — the FP32 pieces of the mixed-precision step form: the PPM
 // face reconstruction (koral/fv/recon.zig:107, C finite.c:210, non-uniform
 // widths) on stencil deviations, the LAXF dissipation (koral/fv/laxf.zig:13)
-// and the flux-CT corner averages (koral/sim/ct.zig:38) in single precision.
+// and the flux-CT corner averages (koral/sim/ct.zig:38) in single precision;
+// KC_MIXED takes the LAXF and CT pieces (the reconstruction is a piece of its
+// own: it moves the floor-level accretion rate by 9e-3 over 1000 steps).
 // Everything else — floors, the one-sided fluxes with their metric
 // contractions, p2u, u2p, the implicit solve and the metric cache — stays
 // FP64. The FP64 form does not use this file.

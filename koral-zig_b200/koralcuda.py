@@ -24,7 +24,7 @@ KC_ERR_OOM = 2
 KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
 KC_FP32_PPM, KC_FP32_LAXF, KC_FP32_CT, KC_FP32_FLUX = 2, 4, 8, 16
-KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT, KC_IMPLICIT_SORTED = 0, 1, 2, 3
+KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT, KC_IMPLICIT_SORTED, KC_IMPLICIT_RUNGS = 0, 1, 2, 3, 4
 KC_NPASS = 14
 KC_ERR_TOO_MANY_CELLS = 9
 KC_NOALLOC_MAX_CELLS = 16384
@@ -151,6 +151,7 @@ def lib():
     L.kc_get_stream.argtypes = [vp, P(vp)]
     L.kc_get_launch_count.argtypes = [vp, P(i64)]
     L.kc_harvest_implicit.argtypes = [vp, i64]
+    L.kc_set_harvest_filter.argtypes = [vp, i32]
     L.kc_get_harvest.argtypes = [vp, vp, vp, i64, P(i64)]
     L.kc_guess_fallbacks.argtypes = [vp]
     L.kc_guess_fallbacks.restype = i64
@@ -179,7 +180,8 @@ def lib():
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
               "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune",
               "kc_kdmp_write_header", "kc_kdmp_parse_header", "kc_kdmp_write", "kc_kdmp_load", "kc_kdmp_write_file",
-              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct", "kc_set_face_tiles"]:
+              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct", "kc_set_face_tiles",
+              "kc_set_harvest_filter"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
     return L
@@ -386,6 +388,11 @@ class Sim:
         """Collect (features, targets) of first-rung converged solves from the
         next implicit pass on, up to `capacity` pairs (0 stops)."""
         self._check(self._lib.kc_harvest_implicit(self._h, int(capacity)))
+
+    def set_harvest_filter(self, mode):
+        """0: harvest every first-rung converged solve; 1: only those whose
+        pre-solve state fails the Newton core's first residual test."""
+        self._check(self._lib.kc_set_harvest_filter(self._h, mode))
 
     def get_harvest(self, capacity):
         x = np.empty((capacity, KC_MLP_IN), dtype=np.float32)

@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(128, KC_U2P_MIN_BLOCKS) k_u2p(DevState s, DevS
   s.flags[0 * nc + c] = 0;
   s.flags[1 * nc + c] = 0;
   Geom g;
-  geom_cell(s, ix, iy, iz, g);
+  geom_cell<true>(s, ix, iy, iz, g);  // read once: evict-first in L2
   bool polar = polar_nc > 0 && (iy < polar_nc || iy > s.gr.ny - polar_nc - 1);
   if (polar) {
     double gdetu_inv = 1.0 / g.gdet;
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(128, KC_U2P_MIN_BLOCKS) k_u2p(DevState s, DevS
   check_floors_mhd(pp, g, gam, fl, gc);
   if (gc) atomicAdd(&sc->n_guard, (unsigned long long)gc);
   check_floors_rad(pp, g, rp);
-  store_cell(s.p, nc, c, pp);
+  store_cell<true>(s.p, nc, c, pp);
   s.flags[3 * nc + c] = res.fixup ? 1 : 0;
   s.flags[4 * nc + c] = rr.corrected ? -1 : 0;
   if (res.fixup) atomicOr(&sc->any_hd, 1);

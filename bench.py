@@ -202,7 +202,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2, "sorted": 3, "rungs": 4}
+IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2, "sorted": 3, "rungs": 4, "iters": 5}
 IMPL_METRIC = "implicit M1 solves/s (batched, independent cells)"
 IMPL_UNIT = "solves/s"
 
@@ -659,13 +659,13 @@ def main():
                     help="guess workload: train on the solves whose pre-solve state must iterate (hard) or on all")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
-    ap.add_argument("--implicit-mode", default=None, choices=["per-cell", "compacting", "split", "sorted", "rungs"],
+    ap.add_argument("--implicit-mode", default=None, choices=["per-cell", "compacting", "split", "sorted", "rungs", "iters"],
                     help="implicit solve form: one thread per cell, the persistent lane-refilling state machine, the "
                          "split opening + compacted-ladder pair, or (batch workload only) the per-cell kernel over "
                          "key-sorted cells; default: sorted for --workload implicit, per-cell otherwise")
     args = ap.parse_args()
-    if args.implicit_mode is None:  # sorted is a batch form; the step's default form is per-cell
-        args.implicit_mode = "sorted" if args.workload == "implicit" else "per-cell"
+    if args.implicit_mode is None:  # iters is a batch form; the step's default form is per-cell
+        args.implicit_mode = "iters" if args.workload == "implicit" else "per-cell"
     if args.steps is None:
         args.steps = 3 if args.workload == "implicit" else 20
     rank = int(os.environ.get("RANK", 0))

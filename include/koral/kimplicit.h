@@ -303,29 +303,64 @@ KC_HD void lag_opac(RadState& st, const RadState& st00) {
   st.opac.rad_ross = st00.opac.rad_ross;
 }
 
+// The loop state of the Newton core at the top of an iteration: what a paused
+// solve (RESUME) carries to its next call. iter = iterations done, 0 = not started.
+struct CoreCarry {
+  double uu[NV], pp[NV];
+  RadState state;
+  int fret, iter;
+};
 // C solve_implicit_lab_4dprim Newton core (implicit.zig:642). Returns 1 on
 // success (pp_out written, *iters set), 0 on failure.
-KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, const double pp0in[NV], const Geom& g,
-                             double dt, double gam, const RadParams& rad, const OpacParams& op, double opdamp,
-                             const ImplicitParams& ip, int whichprim, int whicheq, int whichframe, double pp_out[NV],
-                             int* iters_out) {
+// RESUME = false is the reference's core as is. RESUME = true starts from
+// *carry when carry->iter > 0, runs at most `budget` iterations and then, if the
+// solve has not ended, saves its loop state to *carry and returns 2; the
+// iterations run are those of the uninterrupted core, so a solve split over
+// several calls ends exactly as it would in one.
+template <bool RESUME>
+KC_HDN int solve_4dprim_core_t(const double uu00[NV], const RadState& state00, const double pp0in[NV], const Geom& g,
+                               double dt, double gam, const RadParams& rad, const OpacParams& op, double opdamp,
+                               const ImplicitParams& ip, int whichprim, int whicheq, int whichframe, double pp_out[NV],
+                               int* iters_out, CoreCarry* carry, int budget) {
   double uu[NV], pp[NV];
-  for (int i = 0; i < NV; ++i) {
-    uu[i] = uu00[i];
-    pp[i] = pp0in[i];
-  }
   int sh = (whichprim == PRIM_MHD) ? UU : EE;
   double conv = (whicheq == EQ_ENTROPY) ? ip.entrconv : ip.conv;
-  int fret = apply_constraints(pp, uu, uu00, g, gam, rad, ip, whichprim);
   bool slim = whicheq != EQ_ENTROPY;
+  int fret, iter;
   RadState state;
-  fill_rad_state(pp, g, gam, op, !slim, state);
-  if (ip.lag_opac) lag_opac(state, state00);
+  if (RESUME && carry->iter > 0) {
+    for (int i = 0; i < NV; ++i) {
+      uu[i] = carry->uu[i];
+      pp[i] = carry->pp[i];
+    }
+    state = carry->state;
+    fret = carry->fret;
+    iter = carry->iter;
+  } else {
+    for (int i = 0; i < NV; ++i) {
+      uu[i] = uu00[i];
+      pp[i] = pp0in[i];
+    }
+    fret = apply_constraints(pp, uu, uu00, g, gam, rad, ip, whichprim);
+    fill_rad_state(pp, g, gam, op, !slim, state);
+    if (ip.lag_opac) lag_opac(state, state00);
+    iter = 0;
+  }
+  const int stop = RESUME ? iter + budget : 0;
   double f1[4], f2[4], jac[4][4];
-  int iter = 0;
   bool failed = false;
   bool success = false;
   while (true) {
+    if (RESUME && iter >= stop) {
+      for (int i = 0; i < NV; ++i) {
+        carry->uu[i] = uu[i];
+        carry->pp[i] = pp[i];
+      }
+      carry->state = state;
+      carry->fret = fret;
+      carry->iter = iter;
+      return 2;
+    }
     iter += 1;
     double ppp[NV];
     for (int i = 0; i < NV; ++i) ppp[i] = pp[i];
@@ -439,6 +474,15 @@ KC_HDN int solve_4dprim_core(const double uu00[NV], const RadState& state00, con
   for (int i = 0; i < NV; ++i) pp_out[i] = pp[i];
   *iters_out = iter;
   return 1;
+}
+// the reference's core (koral/solve/implicit.zig:642): 1 on success (pp_out,
+// *iters_out written), 0 on failure
+KC_HD int solve_4dprim_core(const double uu00[NV], const RadState& state00, const double pp0in[NV], const Geom& g,
+                            double dt, double gam, const RadParams& rad, const OpacParams& op, double opdamp,
+                            const ImplicitParams& ip, int whichprim, int whicheq, int whichframe, double pp_out[NV],
+                            int* iters_out) {
+  return solve_4dprim_core_t<false>(uu00, state00, pp0in, g, dt, gam, rad, op, opdamp, ip, whichprim, whicheq,
+                                    whichframe, pp_out, iters_out, nullptr, 0);
 }
 
 // The per-solve preamble of C solve_implicit_lab (implicit.zig:927-961): the

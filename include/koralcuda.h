@@ -69,13 +69,16 @@ enum { KC_GUESS_PLAIN = 0, KC_GUESS_MLP = 1 };
  * the cells sorted by start fluid, optical depth and temperature; RUNGS (the
  * batch entry points only) the sorted cells prepared once (warm start and
  * reference state), then one launch per rung of the ladder over the cells the
- * earlier rungs left unsolved, compacted between rungs */
+ * earlier rungs left unsolved, compacted between rungs; ITERS (the batch entry
+ * points only) as RUNGS, with every rung run in launches of at most 8 Newton
+ * iterations per cell, the cells still iterating compacted between launches */
 enum {
   KC_IMPLICIT_PER_CELL = 0,
   KC_IMPLICIT_COMPACTING = 1,
   KC_IMPLICIT_SPLIT = 2,
   KC_IMPLICIT_SORTED = 3,
-  KC_IMPLICIT_RUNGS = 4
+  KC_IMPLICIT_RUNGS = 4,
+  KC_IMPLICIT_ITERS = 5
 };
 
 /* Pass ids of the per-pass timers, the members of koral/sim/timers.zig:4

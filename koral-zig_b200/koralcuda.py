@@ -25,6 +25,7 @@ KC_BC_PERIODIC, KC_BC_COPY, KC_BC_PUFFY = 0, 1, 2
 KC_PLAIN_FP64, KC_MIXED = 0, 1
 KC_FP32_PPM, KC_FP32_LAXF, KC_FP32_CT, KC_FP32_FLUX = 2, 4, 8, 16
 KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING, KC_IMPLICIT_SPLIT, KC_IMPLICIT_SORTED, KC_IMPLICIT_RUNGS = 0, 1, 2, 3, 4
+KC_IMPLICIT_ITERS = 5
 KC_NPASS = 14
 KC_ERR_TOO_MANY_CELLS = 9
 KC_NOALLOC_MAX_CELLS = 16384

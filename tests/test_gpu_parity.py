@@ -22,7 +22,7 @@ def _kc():
 
 
 MODES = [0, 1, 2]  # KC_IMPLICIT_PER_CELL, KC_IMPLICIT_COMPACTING (persistent state machine), KC_IMPLICIT_SPLIT
-BATCH_MODES = [0, 1, 3, 4]  # the batch entry points: per-cell, persistent, sorted, rung-compacted
+BATCH_MODES = [0, 1, 3, 4, 5]  # the batch entry points: per-cell, persistent, sorted, rung- and iteration-compacted
 
 
 @pytest.mark.parametrize("mode", BATCH_MODES)

@@ -203,6 +203,21 @@ def run_reference(args, rank, world):
 
 
 IMPLICIT_MODES = {"per-cell": 0, "compacting": 1, "split": 2, "sorted": 3, "rungs": 4, "iters": 5}
+
+
+def batch_launches(opt, mode):
+    """The engine's own kernel launches in one kc_implicit_batch call (the radix
+    sort of the sorted forms runs CUB's kernels, not counted): the key kernel,
+    the preparation and one launch per rung, or per rung and round of at most
+    8 Newton iterations (the schedule of launch_iters in kc_abi_batch.inc)."""
+    nrung = 6 * (opt.radimp_opdamp_maxlevels + 1)
+    if mode in (0, 1):
+        return 1
+    if mode == 3:
+        return 2
+    if mode == 4:
+        return 2 + nrung
+    return 2 + nrung * (-(-(opt.radimp_maxiter + 1) // 8))
 IMPL_METRIC = "implicit M1 solves/s (batched, independent cells)"
 IMPL_UNIT = "solves/s"
 
@@ -364,7 +379,7 @@ def run_implicit(args, rank, world, local):
         "roofline": {"bound": "hbm", "kernel": "k_implicit_batch", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                      "algorithmic_bytes": bpc * n},
-        "clocks": clk, "gpu_launches": args.steps,
+        "clocks": clk, "gpu_launches": args.steps * batch_launches(opt, IMPLICIT_MODES[args.implicit_mode]),
     }
     line["reference_battery"] = implicit_battery(kc, opt, stream)
     if rank == 0 and not args.no_cpu_baseline:

@@ -130,7 +130,8 @@ KC_HD Faces reconstruct(int scheme, const double u[5], const double dx[5], doubl
 
 // C f_flux_prime (koral/physics/flux.zig:40). Returns E_NANFLUX on a
 // non-finite flux.
-KC_HDN int f_flux_prime(const double pp[NV], int idim, const Geom& g, double gam, double ff[NV]) {
+// (the body, inlined by kernels that keep its arrays in registers)
+KC_HD int f_flux_prime_inl(const double pp[NV], int idim, const Geom& g, double gam, double ff[NV]) {
   double gdetu = g.gdet;
   double rho = pp[RHO], ugas = pp[UU], s = pp[ENTR];
   double vcon[4] = {0.0, pp[VX], pp[VY], pp[VZ]};
@@ -166,6 +167,7 @@ KC_HDN int f_flux_prime(const double pp[NV], int idim, const Geom& g, double gam
     if (!kmath::isfinite(ff[i])) return E_NANFLUX;
   return E_OK;
 }
+KC_HDN int f_flux_prime(const double pp[NV], int idim, const Geom& g, double gam, double ff[NV]) { return f_flux_prime_inl(pp, idim, g, gam, ff); }
 
 // Lax-Friedrichs, koral/fv/laxf.zig:13
 KC_HD double laxf(double fl, double fr, double ul, double ur, double ag) { return 0.5 * (fr + fl - ag * (ur - ul)); }

@@ -98,7 +98,8 @@ KC_HD bool w_out_of_bounds(double W, double Qtsq, double QdotBsq, double Bsq, co
 }
 
 // C u2p_solver_W (invert.zig:240). pp is in/out (the Newton seed).
-KC_HDN int u2p_solver_w(const double uu[NV], double pp[NV], const Geom& g, int etype, double pgamma) {
+// (the body, inlined by kernels that keep its arrays in registers)
+KC_HD int u2p_solver_w_inl(const double uu[NV], double pp[NV], const Geom& g, int etype, double pgamma) {
   const double conv = 1.0e-10;
   const double big = 1.0 / 1.0e-80;
   double gdetu_inv = 1.0 / g.gdet;
@@ -208,6 +209,9 @@ KC_HDN int u2p_solver_w(const double uu[NV], double pp[NV], const Geom& g, int e
   pp[B3] = uu[B3] * gdetu_inv;
   return 0;
 }
+KC_HDN int u2p_solver_w(const double uu[NV], double pp[NV], const Geom& g, int etype, double pgamma) {
+  return u2p_solver_w_inl(uu, pp, g, etype, pgamma);
+}
 
 struct U2pMhdRes {
   int ret;
@@ -215,7 +219,10 @@ struct U2pMhdRes {
   bool fixup;
 };
 // MHD part of C's u2p cascade (invert.zig:422)
-KC_HDM U2pMhdRes u2p_mhd(const double uu_in[NV], double pp[NV], const Geom& g, double pgamma, const FloorParams& fl) {
+// INL: both W solves (hot energy, entropy fallback) inlined, so the kernel keeps
+// the conserved and primitive arrays in registers instead of a call frame
+template <bool INL>
+KC_HDM U2pMhdRes u2p_mhd_t(const double uu_in[NV], double pp[NV], const Geom& g, double pgamma, const FloorParams& fl) {
   double uu[NV], ppbak[NV], ppmhd[NV];
   for (int i = 0; i < NV; ++i) {
     uu[i] = uu_in[i];
@@ -230,11 +237,11 @@ KC_HDM U2pMhdRes u2p_mhd(const double uu_in[NV], double pp[NV], const Geom& g, d
     uu[RHO] = fl.rhofloor * gdetu / g.alpha;
     ret = -2;
   }
-  int u2pret = u2p_solver_w(uu, ppmhd, g, ETYPE_HOT, pgamma);
+  int u2pret = INL ? u2p_solver_w_inl(uu, ppmhd, g, ETYPE_HOT, pgamma) : u2p_solver_w(uu, ppmhd, g, ETYPE_HOT, pgamma);
   if (u2pret < 0) {
     ret = -1;
     entropy_used = true;
-    u2pret = u2p_solver_w(uu, ppmhd, g, ETYPE_ENTROPY, pgamma);
+    u2pret = INL ? u2p_solver_w_inl(uu, ppmhd, g, ETYPE_ENTROPY, pgamma) : u2p_solver_w(uu, ppmhd, g, ETYPE_ENTROPY, pgamma);
     if (u2pret < 0) ret = -2;
   }
   if (u2pret >= 0) {
@@ -249,11 +256,15 @@ KC_HDM U2pMhdRes u2p_mhd(const double uu_in[NV], double pp[NV], const Geom& g, d
   r.fixup = ret < -1;
   return r;
 }
+KC_HDM U2pMhdRes u2p_mhd(const double uu_in[NV], double pp[NV], const Geom& g, double pgamma, const FloorParams& fl) {
+  return u2p_mhd_t<false>(uu_in, pp, g, pgamma, fl);
+}
 
 // C check_floors_mhd, DRIFTFRAME (invert.zig:474). Returns -1 if floored.
 // guard_count is incremented when a drift-frame guard diverted the algebra
 // (the reference's n_guard_recoveries, invert.zig:44).
-KC_HDN int check_floors_mhd(double pp[NV], const Geom& g, double pgamma, const FloorParams& fl, int& guard_count) {
+// (the body, inlined by kernels that keep its arrays in registers)
+KC_HD int check_floors_mhd_inl(double pp[NV], const Geom& g, double pgamma, const FloorParams& fl, int& guard_count) {
   int ret = 0;
   if (pp[RHO] < fl.rhofloor) {
     pp[RHO] = fl.rhofloor;
@@ -366,6 +377,7 @@ KC_HDN int check_floors_mhd(double pp[NV], const Geom& g, double pgamma, const F
   if (ret < 0) pp[ENTR] = s_from_u(pp[RHO], pp[UU], pgamma);
   return ret;
 }
+KC_HDN int check_floors_mhd(double pp[NV], const Geom& g, double pgamma, const FloorParams& fl, int& guard_count) { return check_floors_mhd_inl(pp, g, pgamma, fl, guard_count); }
 
 // ---- M1 radiation (koral/physics/radiation.zig) ----------------------------
 // R^mu nu of the M1 closure (radiation.zig:79, C calc_Rij_M1)
@@ -462,7 +474,8 @@ struct U2pRadRes {
   bool corrected;
 };
 // C u2p_rad (invert_rad.zig:189). Writes pp[EE..FZ] on success.
-KC_HDN U2pRadRes u2p_rad(const double uu[NV], double pp[NV], const Geom& g, const RadParams& rp) {
+// (the body, inlined by kernels that keep its arrays in registers)
+KC_HD U2pRadRes u2p_rad_inl(const double uu[NV], double pp[NV], const Geom& g, const RadParams& rp) {
   const double gsl = 1.0 - 1e-10;
   const double numepsilon = 2.220446049250313e-16;
   double gdetu = g.gdet;
@@ -513,6 +526,7 @@ KC_HDN U2pRadRes u2p_rad(const double uu[NV], double pp[NV], const Geom& g, cons
   res.corrected = corrected;
   return res;
 }
+KC_HDN U2pRadRes u2p_rad(const double uu[NV], double pp[NV], const Geom& g, const RadParams& rp) { return u2p_rad_inl(uu, pp, g, rp); }
 
 // C check_floors_rad (invert_rad.zig:266)
 KC_HDM int check_floors_rad(double pp[NV], const Geom& g, const RadParams& rp) {

@@ -674,6 +674,8 @@ def main():
                     help="guess workload: train on the solves whose pre-solve state must iterate (hard) or on all")
     ap.add_argument("--train-steps", type=int, default=3000, help="training minibatches of the guess workload")
     ap.add_argument("--cells", type=int, default=1 << 22, help="cells of the implicit microbenchmark")
+    ap.add_argument("--face-tiles", type=int, default=None, choices=[0, 1, 2],
+                    help="form of the y and z face sweeps (kc_set_face_tiles); default: the engine's")
     ap.add_argument("--implicit-mode", default=None, choices=["per-cell", "compacting", "split", "sorted", "rungs", "iters"],
                     help="implicit solve form: one thread per cell, the persistent lane-refilling state machine, the "
                          "split opening + compacted-ladder pair, or (batch workload only) the per-cell kernel over "
@@ -723,6 +725,8 @@ def main():
     t0 = time.perf_counter()
     fac = sim.initPuffy(1e-3, 1e-3, args.seed)
     init_s = time.perf_counter() - t0
+    if args.face_tiles is not None:
+        sim.set_face_tiles(args.face_tiles)
     if args.graph:
         sim.set_graph(True)
     for _ in range(args.warmup):

@@ -11,10 +11,11 @@
 
 // Resident blocks of 128 per SM that the register budgets of the u2p, radiative
 // viscosity, dynamo and boundary kernels must allow (1: uncapped). Measured on
-// the wedge: 3 (168 registers) makes u2p 5% and the dynamo 4% faster, and the
-// boundary kernel 3% slower; the viscosity kernel is indifferent.
+// the wedge: 3 (168 registers) makes the dynamo 4% faster and the boundary kernel
+// 3% slower; the viscosity kernel is indifferent. The u2p kernel with its
+// inversion inlined: 4 (128 registers, 16 warps per SM) 4% faster than 3.
 #ifndef KC_U2P_MIN_BLOCKS
-#define KC_U2P_MIN_BLOCKS 3
+#define KC_U2P_MIN_BLOCKS 4
 #endif
 #ifndef KC_RIJVISC_MIN_BLOCKS
 #define KC_RIJVISC_MIN_BLOCKS 1
@@ -829,8 +830,9 @@ __device__ int face_state(const DevState& s, DevScalars* sc, const FluxArgs& a, 
 }
 #ifndef KC_FLUX_MIN_BLOCKS
 // resident blocks of 128 per SM the face kernel's register budget must allow:
-// 3 caps it at 168 registers (194 uncapped), measured 14% faster; 4 (128) 10%
-#define KC_FLUX_MIN_BLOCKS 3
+// with the floors and the flux inlined, 4 (128 registers, 16 warps per SM)
+// measured 10% faster than 3 (168) and 2 (206, no spills) 29% slower
+#define KC_FLUX_MIN_BLOCKS 4
 #endif
 // MIXED: the instance of the mixed form, whose FP32 pieces (reconstruction,
 // LAXF dissipation, rounded fluxes; kc_mixed.cuh) FluxArgs::fp32 selects
@@ -1186,56 +1188,79 @@ template <int FORM, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
                                                             ImplExtra x) {
   const double dt = s.coef[a.dt_slot];
-  long ix, iy, iz;
+  long ix = 0, iy = 0, iz = 0;
+  bool act;
   if (a.phi_fastest) {
-    if (!domain_cell_phi_fastest(s.gr, ix, iy, iz)) return;
+    act = domain_cell_phi_fastest(s.gr, ix, iy, iz);
   } else if (a.y_fastest) {
     // 2D: neighbours in theta at one radius (measured 10% faster than x fastest
     // on the 384x360 grid; 8 x 4 tiles per warp were in between)
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)s.gr.nx * s.gr.ny * s.gr.nz) return;
-    iy = t % s.gr.ny;
-    long q = t / s.gr.ny;
-    ix = q % s.gr.nx;
-    iz = q / s.gr.nx;
+    act = t < (long)s.gr.nx * s.gr.ny * s.gr.nz;
+    if (act) {
+      iy = t % s.gr.ny;
+      long q = t / s.gr.ny;
+      ix = q % s.gr.nx;
+      iz = q / s.gr.nx;
+    }
   } else {
     Range r = {0, 0, 0, s.gr.nx, s.gr.ny, s.gr.nz};
-    if (!range_cell(r, ix, iy, iz)) return;
+    act = range_cell(r, ix, iy, iz);
   }
-  if (a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) return;
-  long nc = s.gr.nc, c = cidx(s.gr, ix, iy, iz);
+  if (act && a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) act = false;
+  // the plain form meets a block barrier below; the other forms leave here
+  if (FORM != IMPL_PLAIN && !act) return;
+  long nc = s.gr.nc, c = act ? cidx(s.gr, ix, iy, iz) : 0;
   // the cell's metric is read once and its state written once: evict-first in
   // L2 (which keeps L2 for the solver's call frames); the state loads stay plain
   // (their evict-first form costs the kernel registers and 200 bytes of spills)
   double uu[NV], pp[NV];
-  load_cell(s.u, nc, c, uu);
-  load_cell(s.p, nc, c, pp);
   Geom g;
-  geom_cell<true>(s, ix, iy, iz, g);
-  double pp00[NV];
-  constexpr bool HARVEST = FORM == IMPL_FULL;
-  if (HARVEST)
-    for (int i = 0; i < NV; ++i) pp00[i] = pp[i];
   ImplicitResult res;
-  if (FORM != IMPL_PLAIN && x.guess) {
-    long nd = (long)s.gr.nx * s.gr.ny * s.gr.nz, td = ix + s.gr.nx * (iy + s.gr.ny * iz);
-    double g0[NV];
-    for (int i = 0; i < NV; ++i) g0[i] = x.guess[i * nd + td];
-    res = solve_implicit_lab_from(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, g0);
-    if (!res.ok) {
-      atomicAdd(x.n_fallback, 1ULL);
+  if constexpr (FORM == IMPL_PLAIN) {
+    // In two phases: every thread of the block runs its warm start (the 1-D
+    // bisection), the block synchronises, then every thread runs its ladder, so
+    // that the warps of a block execute the same part of the solver's code at a
+    // time (the code is far larger than the instruction cache; measured 3.8%
+    // faster than one unsynchronised pass). The arithmetic is solve_implicit_lab's.
+    ImplicitPre pre;
+    if (act) {
+      load_cell(s.u, nc, c, uu);
+      load_cell(s.p, nc, c, pp);
+      geom_cell<true>(s, ix, iy, iz, g);
+      implicit_prepare(pp, g, dt, a.gam, a.op, a.ip, pre);
+    }
+    __syncthreads();
+    if (!act) return;
+    res = implicit_ladder(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, pre);
+  } else {
+    load_cell(s.u, nc, c, uu);
+    load_cell(s.p, nc, c, pp);
+    geom_cell<true>(s, ix, iy, iz, g);
+    double pp00[NV];
+    constexpr bool HARVEST = FORM == IMPL_FULL;
+    if (HARVEST)
+      for (int i = 0; i < NV; ++i) pp00[i] = pp[i];
+    if (x.guess) {
+      long nd = (long)s.gr.nx * s.gr.ny * s.gr.nz, td = ix + s.gr.nx * (iy + s.gr.ny * iz);
+      double g0[NV];
+      for (int i = 0; i < NV; ++i) g0[i] = x.guess[i * nd + td];
+      res = solve_implicit_lab_from(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, g0);
+      if (!res.ok) {
+        atomicAdd(x.n_fallback, 1ULL);
+        res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
+      }
+    } else {
       res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
     }
-  } else {
-    res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
-  }
-  if (HARVEST && x.hx && res.ok && res.rung == 0 && (!x.hfilter || presolve_needs_newton(pp00, g, dt, a))) {
-    unsigned long long k = atomicAdd(x.hcount, 1ULL);
-    if ((long)k < x.hcap) {
-      double ehat = -calc_ff_rtt(pp00, g, nullptr);
-      int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
-      mlp_features_raw(pp00, dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
-      mlp_targets_raw(pp00, pp, sw, x.ht + k * MLP_OUT);
+    if (HARVEST && x.hx && res.ok && res.rung == 0 && (!x.hfilter || presolve_needs_newton(pp00, g, dt, a))) {
+      unsigned long long k = atomicAdd(x.hcount, 1ULL);
+      if ((long)k < x.hcap) {
+        double ehat = -calc_ff_rtt(pp00, g, nullptr);
+        int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
+        mlp_features_raw(pp00, dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
+        mlp_targets_raw(pp00, pp, sw, x.ht + k * MLP_OUT);
+      }
     }
   }
   if (res.ok) {

@@ -581,7 +581,7 @@ void launch_dynamo(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   PassScope ps(h, KC_PASS_DYNAMO);
   ++h->n_launch;
-  k_scale_height<<<nblk(gr.nx, SH_WARPS), SH_WARPS * 32, 0, h->stream>>>(h->ds);
+  k_scale_height<<<(unsigned)gr.nx, SH_THREADS, 0, h->stream>>>(h->ds);
   launch_set_bc(h);
   DynArgs a;
   a.gam = h->sp.gam;
@@ -1147,7 +1147,7 @@ int kc_scalars(kc_handle* h, double dt, double r_lum, double r_scale, kc_scalar_
   // scale height: the dynamo's per-radius fold (dynamo.zig:239), into a scratch row
   DevState ds2 = h->ds;
   ds2.scaleth = scaleth;
-  k_scale_height<<<nblk(gr.nx, SH_WARPS), SH_WARPS * 32, 0, h->stream>>>(ds2);
+  k_scale_height<<<(unsigned)gr.nx, SH_THREADS, 0, h->stream>>>(ds2);
   k_init_beta_max<<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, h->sp.gam);
   double hres[10], hsh = 0.0;
   DevScalars z;

@@ -1518,21 +1518,21 @@ __global__ void __launch_bounds__(128, KC_RIJVISC_MIN_BLOCKS) k_rijvisc(DevState
 // ---- mimic dynamo (koral/sim/dynamo.zig) --------------------------------------
 // Per-radius scale height (dynamo.zig:158 calcScaleHeight). The fold over
 // (iy, iz) of each x column keeps the reference's serial order (iy outer, iz
-// inner). One warp per column: the lanes load and form 32 consecutive terms
-// (rho gdet and rho gdet dtheta^2) at a time, and every lane then folds those
-// 32 terms in order from shuffles, so the sums are the serial ones and the
-// loads of a chunk overlap; the columns run in parallel across the SMs.
-constexpr int SH_WARPS = 2;
-__global__ void __launch_bounds__(SH_WARPS * 32) k_scale_height(DevState s) {
-  const unsigned full = 0xffffffffu;
-  int lane = threadIdx.x & 31;
-  long ix = (long)blockIdx.x * SH_WARPS + (threadIdx.x >> 5);
-  if (ix >= s.gr.nx) return;  // whole warps leave together
-  long nz = s.gr.nz, nsteps = (long)s.gr.ny * nz, nc = s.gr.nc;
-  double sigma = 0.0, sth = 0.0;
-  for (long k0 = 0; k0 < nsteps; k0 += 32) {
-    long k = k0 + lane;
-    double a = 0.0, b = 0.0;
+// inner). One block per column: its threads form SH_THREADS consecutive terms
+// (rho gdet and rho gdet dtheta^2) at a time into shared memory, and thread 0
+// folds them in order, so the sums are the serial ones; the terms of the next
+// chunk are loaded while thread 0 folds the current one (two buffers), and the
+// columns run in parallel across the SMs.
+constexpr int SH_THREADS = 512;
+__global__ void __launch_bounds__(SH_THREADS) k_scale_height(DevState s) {
+  __shared__ double ta[2][SH_THREADS], tb[2][SH_THREADS];
+  const long ix = blockIdx.x;
+  const int t = threadIdx.x;
+  const long nz = s.gr.nz, nsteps = (long)s.gr.ny * nz, nc = s.gr.nc;
+  const long nch = (nsteps + SH_THREADS - 1) / SH_THREADS;
+  auto term = [&](long k, double& a, double& b) {
+    a = 0.0;
+    b = 0.0;
     if (k < nsteps) {
       long c = cidx(s.gr, ix, k / nz, k % nz);
       double rho = s.p[RHO * nc + c], gd = s.cgc[10L * nc + c];
@@ -1540,14 +1540,32 @@ __global__ void __launch_bounds__(SH_WARPS * 32) k_scale_height(DevState s) {
       a = rho * gd;
       b = rho * gd * dth * dth;
     }
-    int m = nsteps - k0 < 32 ? (int)(nsteps - k0) : 32;
-    for (int j = 0; j < m; ++j) {
-      double aj = __shfl_sync(full, a, j), bj = __shfl_sync(full, b, j);
-      sigma += aj;
-      sth += bj;
+  };
+  double a, b;
+  term(t, a, b);
+  ta[0][t] = a;
+  tb[0][t] = b;
+  __syncthreads();
+  double sigma = 0.0, sth = 0.0;  // thread 0's
+  for (long ch = 0; ch < nch; ++ch) {
+    const int buf = (int)(ch & 1);
+    const bool next = ch + 1 < nch;
+    if (next) term((ch + 1) * SH_THREADS + t, a, b);  // in flight during the fold
+    if (t == 0) {
+      const long m = nsteps - ch * SH_THREADS < SH_THREADS ? nsteps - ch * SH_THREADS : SH_THREADS;
+#pragma unroll 8
+      for (int j = 0; j < m; ++j) {
+        sigma += ta[buf][j];
+        sth += tb[buf][j];
+      }
     }
+    if (next) {
+      ta[buf ^ 1][t] = a;
+      tb[buf ^ 1][t] = b;
+    }
+    __syncthreads();
   }
-  if (lane == 0) s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
+  if (t == 0) s.scaleth[ix] = (ix > 0) ? kmath::sqrt(sth / sigma) : sth;
 }
 struct DynArgs {
   double gam, a, rhor, risco;

@@ -613,10 +613,14 @@ KC_HDN int implicit_first_exit(double uu[NV], double pp[NV], const Geom& g, doub
 // smaller first-rung residual (starting every such cell from the learned
 // state measured slower: the prediction is worse than the pre-solve state for
 // a part of them).
-KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
-                                              const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
-                                              const double guess[NV]) {
-  ImplicitPre pre;
+// The learned start's preamble: the reference conserveds and state of the
+// pre-solve primitives, the start fluid, and the core's first exit on rung 0
+// (lab frame, energy equation) at the pre-solve state; returns 1 when that exit
+// is taken (uu, pp written), else 0 with pre.pp0 the one of the pre-solve and
+// the learned state that has the smaller rung-0 first residual.
+KC_HDN int implicit_prepare_from(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
+                                 const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
+                                 const double guess[NV], ImplicitPre& pre) {
   p2u(pp, pre.uu00, g, gam);
   double ehat = -calc_ff_rtt(pp, g, nullptr);
   fill_rad_state(pp, g, gam, op, true, pre.state00);
@@ -624,21 +628,31 @@ KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], cons
   double pc[NV];
   double e0 = implicit_start_residual(pre.uu00, pre.state00, pp, g, dt, gam, rad, op, 1.0, ip, pre.startwith, pc);
   if (e0 < ip.conv) {
-    // the core's first exit on rung 0 (lab frame, energy equation)
-    ImplicitResult res;
     for (int i = 0; i < NV; ++i) pp[i] = pc[i];
     p2u(pc, uu, g, gam);
-    res.ok = 1;
-    res.rung = 0;
-    res.iters = 1;
-    res.whichprim = pre.startwith;
-    res.whicheq = EQ_ENERGY;
-    res.whichframe = FRAME_LAB;
-    return res;
+    return 1;
   }
   double e1 = implicit_start_residual(pre.uu00, pre.state00, guess, g, dt, gam, rad, op, 1.0, ip, pre.startwith, pc);
   bool learned = e1 < e0;
   for (int i = 0; i < NV; ++i) pre.pp0[i] = learned ? guess[i] : pp[i];
+  return 0;
+}
+// the result of the core's first exit on rung 0
+KC_HD ImplicitResult implicit_first_exit_result(int startwith) {
+  ImplicitResult res;
+  res.ok = 1;
+  res.rung = 0;
+  res.iters = 1;
+  res.whichprim = startwith;
+  res.whicheq = EQ_ENERGY;
+  res.whichframe = FRAME_LAB;
+  return res;
+}
+KC_HDN ImplicitResult solve_implicit_lab_from(double uu[NV], double pp[NV], const Geom& g, double dt, double gam,
+                                              const RadParams& rad, const OpacParams& op, const ImplicitParams& ip,
+                                              const double guess[NV]) {
+  ImplicitPre pre;
+  if (implicit_prepare_from(uu, pp, g, dt, gam, rad, op, ip, guess, pre)) return implicit_first_exit_result(pre.startwith);
   return implicit_ladder(uu, pp, g, dt, gam, rad, op, ip, pre);
 }
 

@@ -275,19 +275,19 @@ int kc_set_face_tiles(kc_handle* h, int32_t mode);
 
 /* The autotuner's choice (no reference counterpart): implicit form
  * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT), threads per block of the
- * per-cell implicit, face-flux and u2p kernels, and the per-cell implicit
- * kernel's thread -> cell order (1, the default: phi fastest on 3D grids, so
- * that a warp's cells share r and theta, theta fastest on 2D grids; 0: x
- * fastest), its register budget (resident blocks of 128 threads per SM: 2
- * with 255 registers per thread, 3 with 168) and whether the y and z face
- * sweeps stage their PPM stencils in shared-memory tiles, with the measured
- * step time of the choice and of the configuration on entry. */
+ * per-cell implicit kernel (one block per SM: 256 threads with 255 registers
+ * each, 384 with 168, 512 with 128), of the face-flux and of the u2p kernels,
+ * the per-cell implicit kernel's thread -> cell order (1, the default: phi
+ * fastest on 3D grids, so that a warp's cells share r and theta, theta fastest
+ * on 2D grids; 0: x fastest) and whether the y and z face sweeps stage their
+ * PPM stencils in shared-memory tiles, with the measured step time of the
+ * choice and of the configuration on entry. */
 typedef struct kc_tune_result {
   int32_t implicit_mode, tpb_implicit, tpb_flux, tpb_u2p;
   double ms_per_step, ms_per_step_entry;
   int32_t trials;
   int32_t implicit_phi_fastest;
-  int32_t implicit_min_blocks; /* 2: 255 registers per thread, 3: 168; 0: by cell order */
+  int32_t implicit_warps; /* warps per SM of the per-cell implicit kernel: tpb_implicit / 32 */
   int32_t face_tiles;          /* the y and z face sweeps' form (kc_set_face_tiles) */
 } kc_tune_result;
 /* Times whole steps on the handle's current state for each candidate, one

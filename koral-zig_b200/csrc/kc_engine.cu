@@ -64,8 +64,10 @@ struct kc_handle {
   double min_dx = 0, min_dy = 0, min_dz = 0;
   int impl_blocks = 0;  // resident blocks of the persistent implicit kernel
   double* init_dv = nullptr;  // the PUFFY init's per-column torus profile
-  // block sizes of the per-cell implicit, face-flux and u2p kernels (kc_autotune)
-  int tpb_implicit = TPB, tpb_flux = TPB, tpb_u2p = TPB;
+  // block sizes of the per-cell implicit, face-flux and u2p kernels (kc_autotune);
+  // the implicit kernel's block fills an SM: 256 (255 registers), 384 (168) or
+  // 512 threads (128)
+  int tpb_implicit = KC_IMPLICIT_TPB, tpb_flux = TPB, tpb_u2p = TPB;
 #ifndef KC_IMPLICIT_PHI_FASTEST
 #define KC_IMPLICIT_PHI_FASTEST 1
 #endif
@@ -76,9 +78,6 @@ struct kc_handle {
   // phi fastest (warps of cells sharing r and theta) or x fastest; for the
   // implicit kernel on 2D grids the same switch selects theta fastest
   int implicit_phi_fastest = KC_IMPLICIT_PHI_FASTEST, u2p_phi_fastest = KC_U2P_PHI_FASTEST;
-  // resident blocks of 128 per SM the per-cell implicit kernel's registers allow:
-  // 2 (255 registers) or 3 (168); 0 picks by cell order (2 when phi is fastest)
-  int implicit_min_blocks = 0;
   // the y and z face sweeps of the plain form: 0 one thread per face with its own
   // two PPMs, 1 tiles with the reconstructed faces in shared memory, 2 tiles that
   // also stage the stencil rows in shared memory
@@ -395,11 +394,6 @@ int ensure_split(kc_handle* h) {
   return KC_OK;
 }
 
-int implicit_blocks(const kc_handle* h, const ImplArgs& a) {
-  if (h->implicit_min_blocks) return h->implicit_min_blocks;
-  return a.phi_fastest ? 2 : 3;
-}
-
 void launch_implicit(kc_handle* h, int dt_slot) {
   const DGrid& gr = h->gr;
   ImplArgs a;
@@ -460,12 +454,15 @@ void launch_implicit(kc_handle* h, int dt_slot) {
     x.guess = h->guess;
   }
   ++h->n_launch;
-  unsigned nb = nblk(ndom, h->tpb_implicit);
-  if (h->hcap > 0) k_implicit<IMPL_FULL, 2><<<nblk(ndom), TPB, 0, h->stream>>>(h->ds, h->dsc, a, x);
-  else if (extra) k_implicit<IMPL_GUESS, 2><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
-  else if (implicit_blocks(h, a) == 2)
-    k_implicit<IMPL_PLAIN, 2><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
-  else k_implicit<IMPL_PLAIN, 3><<<nb, h->tpb_implicit, 0, h->stream>>>(h->ds, h->dsc, a, x);
+  // one block per SM; the learned-guess and harvest forms in the default block
+  const int nt = extra || (h->tpb_implicit != 256 && h->tpb_implicit != 512) ? KC_IMPLICIT_TPB : h->tpb_implicit;
+  const unsigned nb = nblk(ndom, nt);
+  cudaStream_t st = h->stream;
+  if (h->hcap > 0) k_implicit<IMPL_FULL, KC_IMPLICIT_TPB><<<nb, nt, 0, st>>>(h->ds, h->dsc, a, x);
+  else if (extra) k_implicit<IMPL_GUESS, KC_IMPLICIT_TPB><<<nb, nt, 0, st>>>(h->ds, h->dsc, a, x);
+  else if (nt == 256) k_implicit<IMPL_PLAIN, 256><<<nb, nt, 0, st>>>(h->ds, h->dsc, a, x);
+  else if (nt == 512) k_implicit<IMPL_PLAIN, 512><<<nb, nt, 0, st>>>(h->ds, h->dsc, a, x);
+  else k_implicit<IMPL_PLAIN, KC_IMPLICIT_TPB><<<nb, nt, 0, st>>>(h->ds, h->dsc, a, x);
 }
 
 void launch_wavespeeds(kc_handle* h) {

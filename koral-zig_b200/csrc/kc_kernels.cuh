@@ -1180,15 +1180,24 @@ __device__ __noinline__ bool presolve_needs_newton(const double pp00[NV], const 
 // not compiled into it, so its registers and code size are those of the plain
 // solve); IMPL_GUESS adds the learned start only; IMPL_FULL the learned start
 // and the training-pair harvest.
-// MINB: resident blocks of 128 per SM that the register budget must allow.
-// With the x-fastest cell order (2D grids) 3 (168 registers, 12 warps per SM)
-// measured 2-3% faster than 255 registers (8 warps); with the phi-fastest order
-// of 3D grids, whose warps walk the solver together, 255 registers measured 6%
-// faster than 168 and 128 slower still. The host picks the instance by order.
+// NT: threads per block, and one block per SM: the register budget follows
+// (256 threads: 255 registers, 8 warps; 384: 168, 12 warps; 512: 128, 16 warps;
+// an SM sub-partition holds 16 K registers, so no budget between these gives
+// more warps). Every form runs in two block-synchronous phases: every thread's
+// warm start (the 1-D bisection, or the learned start's pick), a block barrier,
+// then every thread's ladder, so that all warps of the SM execute the same part
+// of the solver's code at a time (the code is far larger than the instruction
+// cache). Measured on the 192x180x64 wedge, implicit pass per step: one
+// unsynchronised pass in blocks of 128 58.1 ms (255 registers, 2 blocks per SM);
+// the two phases in blocks of 128 56.4; SM-wide blocks of 256 50.2, of 384 46.0,
+// of 512 48.2; a third phase (the rung-0 first residual test) 52.9 at 256.
 enum : int { IMPL_PLAIN = 0, IMPL_GUESS = 1, IMPL_FULL = 2 };
-template <int FORM, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
-                                                            ImplExtra x) {
+#ifndef KC_IMPLICIT_TPB
+#define KC_IMPLICIT_TPB 384  // the default block: 12 warps, 168 registers
+#endif
+template <int FORM, int NT>
+__global__ void __launch_bounds__(NT, 1) k_implicit(DevState s, DevScalars* sc, const __grid_constant__ ImplArgs a,
+                                                        ImplExtra x) {
   const double dt = s.coef[a.dt_slot];
   long ix = 0, iy = 0, iz = 0;
   bool act;
@@ -1210,59 +1219,50 @@ __global__ void __launch_bounds__(128, MINB) k_implicit(DevState s, DevScalars* 
     act = range_cell(r, ix, iy, iz);
   }
   if (act && a.polar_nc > 0 && (iy < a.polar_nc || iy > s.gr.ny - a.polar_nc - 1)) act = false;
-  // the plain form meets a block barrier below; the other forms leave here
-  if (FORM != IMPL_PLAIN && !act) return;
   long nc = s.gr.nc, c = act ? cidx(s.gr, ix, iy, iz) : 0;
+  constexpr bool HARVEST = FORM == IMPL_FULL;
+  const bool guessed = FORM != IMPL_PLAIN && x.guess != nullptr;
   // the cell's metric is read once and its state written once: evict-first in
   // L2 (which keeps L2 for the solver's call frames); the state loads stay plain
   // (their evict-first form costs the kernel registers and 200 bytes of spills)
-  double uu[NV], pp[NV];
+  double uu[NV], pp[NV], pp00[NV];
   Geom g;
-  ImplicitResult res;
-  if constexpr (FORM == IMPL_PLAIN) {
-    // In two phases: every thread of the block runs its warm start (the 1-D
-    // bisection), the block synchronises, then every thread runs its ladder, so
-    // that the warps of a block execute the same part of the solver's code at a
-    // time (the code is far larger than the instruction cache; measured 3.8%
-    // faster than one unsynchronised pass). The arithmetic is solve_implicit_lab's.
-    ImplicitPre pre;
-    if (act) {
-      load_cell(s.u, nc, c, uu);
-      load_cell(s.p, nc, c, pp);
-      geom_cell<true>(s, ix, iy, iz, g);
-      implicit_prepare(pp, g, dt, a.gam, a.op, a.ip, pre);
-    }
-    __syncthreads();
-    if (!act) return;
-    res = implicit_ladder(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, pre);
-  } else {
+  ImplicitPre pre;
+  int done = 0;  // the learned form's pre-solve state took the core's first exit
+  if (act) {
     load_cell(s.u, nc, c, uu);
     load_cell(s.p, nc, c, pp);
     geom_cell<true>(s, ix, iy, iz, g);
-    double pp00[NV];
-    constexpr bool HARVEST = FORM == IMPL_FULL;
     if (HARVEST)
       for (int i = 0; i < NV; ++i) pp00[i] = pp[i];
-    if (x.guess) {
+    if (guessed) {
       long nd = (long)s.gr.nx * s.gr.ny * s.gr.nz, td = ix + s.gr.nx * (iy + s.gr.ny * iz);
       double g0[NV];
       for (int i = 0; i < NV; ++i) g0[i] = x.guess[i * nd + td];
-      res = solve_implicit_lab_from(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, g0);
-      if (!res.ok) {
-        atomicAdd(x.n_fallback, 1ULL);
-        res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
-      }
+      done = implicit_prepare_from(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, g0, pre);
     } else {
+      implicit_prepare(pp, g, dt, a.gam, a.op, a.ip, pre);
+    }
+  }
+  __syncthreads();
+  if (!act) return;
+  ImplicitResult res;
+  if (done) {
+    res = implicit_first_exit_result(pre.startwith);
+  } else {
+    res = implicit_ladder(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip, pre);
+    if (guessed && !res.ok) {  // the seeded ladder failed: the plain solve
+      atomicAdd(x.n_fallback, 1ULL);
       res = solve_implicit_lab(uu, pp, g, dt, a.gam, a.rp, a.op, a.ip);
     }
-    if (HARVEST && x.hx && res.ok && res.rung == 0 && (!x.hfilter || presolve_needs_newton(pp00, g, dt, a))) {
-      unsigned long long k = atomicAdd(x.hcount, 1ULL);
-      if ((long)k < x.hcap) {
-        double ehat = -calc_ff_rtt(pp00, g, nullptr);
-        int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
-        mlp_features_raw(pp00, dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
-        mlp_targets_raw(pp00, pp, sw, x.ht + k * MLP_OUT);
-      }
+  }
+  if (HARVEST && x.hx && res.ok && res.rung == 0 && (!x.hfilter || presolve_needs_newton(pp00, g, dt, a))) {
+    unsigned long long k = atomicAdd(x.hcount, 1ULL);
+    if ((long)k < x.hcap) {
+      double ehat = -calc_ff_rtt(pp00, g, nullptr);
+      int sw = (ehat < a.ip.threshold * pp00[UU]) ? PRIM_RAD : PRIM_MHD;
+      mlp_features_raw(pp00, dt, g.gdet, g.alpha, sw, x.hx + k * MLP_IN);
+      mlp_targets_raw(pp00, pp, sw, x.ht + k * MLP_OUT);
     }
   }
   if (res.ok) {

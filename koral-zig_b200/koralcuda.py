@@ -93,7 +93,7 @@ class KcTuneResult(ctypes.Structure):
     _fields_ = [("implicit_mode", ctypes.c_int32), ("tpb_implicit", ctypes.c_int32), ("tpb_flux", ctypes.c_int32),
                 ("tpb_u2p", ctypes.c_int32), ("ms_per_step", _d), ("ms_per_step_entry", _d),
                 ("trials", ctypes.c_int32), ("implicit_phi_fastest", ctypes.c_int32),
-                ("implicit_min_blocks", ctypes.c_int32), ("face_tiles", ctypes.c_int32)]
+                ("implicit_warps", ctypes.c_int32), ("face_tiles", ctypes.c_int32)]
 
 
 class KcStepInfo(ctypes.Structure):

@@ -247,7 +247,8 @@ def test_autotune_restores_state_and_keeps_bits():
     p0, c0 = b.p, b.counters()
     r = b.autotune(1)
     assert r["implicit_mode"] in (0, 2) and r["trials"] >= 2
-    for k in ("tpb_implicit", "tpb_flux", "tpb_u2p"):
+    assert r["tpb_implicit"] in (256, 384, 512) and r["implicit_warps"] == r["tpb_implicit"] // 32
+    for k in ("tpb_flux", "tpb_u2p"):
         assert r[k] in (64, 96, 128)
     assert r["implicit_phi_fastest"] in (0, 1)
     assert np.array_equal(b.p, p0) and b.counters() == c0

@@ -272,6 +272,12 @@ int kc_set_graph(kc_handle* h, int32_t on);
  * once into shared memory, 2 the same with the PPM stencil rows staged in
  * shared memory too. kc_autotune picks among them. */
 int kc_set_face_tiles(kc_handle* h, int32_t mode);
+/* Threads per block of the per-cell implicit kernel (no reference counterpart;
+ * every size gives the same bits): one block fills an SM, so the size sets the
+ * register budget: 256 (255 registers per thread, 8 warps), 384 (168, 12 warps;
+ * the default) or 512 (128, 16 warps). Other sizes: KC_ERR_INVALID_CONFIG.
+ * kc_autotune picks among them. */
+int kc_set_implicit_threads(kc_handle* h, int32_t threads);
 
 /* The autotuner's choice (no reference counterpart): implicit form
  * (KC_IMPLICIT_PER_CELL or KC_IMPLICIT_SPLIT), threads per block of the

@@ -1324,6 +1324,14 @@ int kc_set_face_tiles(kc_handle* h, int32_t mode) {
   drop_graph(h);
   return KC_OK;
 }
+int kc_set_implicit_threads(kc_handle* h, int32_t threads) {
+  if (!h) return KC_ERR_INVALID_CONFIG;
+  if (threads != 256 && threads != 384 && threads != 512)
+    return reject(h, KC_ERR_INVALID_CONFIG, "implicit threads per block must be 256, 384 or 512");
+  h->tpb_implicit = threads;
+  drop_graph(h);
+  return KC_OK;
+}
 int kc_set_graph(kc_handle* h, int32_t on) {
   if (!h) return KC_ERR_INVALID_CONFIG;
   if (h->stream) cudaStreamSynchronize(h->stream);

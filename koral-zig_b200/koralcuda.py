@@ -136,6 +136,7 @@ def lib():
     L.kc_set_implicit_mode.argtypes = [vp, i32]
     L.kc_set_graph.argtypes = [vp, i32]
     L.kc_set_face_tiles.argtypes = [vp, i32]
+    L.kc_set_implicit_threads.argtypes = [vp, i32]
     L.kc_autotune.argtypes = [vp, i32, P(KcTuneResult)]
     L.kc_set_guess.argtypes = [vp, i32, vp, i64]
     L.kc_init_puffy.argtypes = [vp, dbl, dbl, ctypes.c_uint64, P(dbl)]
@@ -181,7 +182,7 @@ def lib():
               "kc_synth_implicit_cells", "kc_scalars", "kc_harvest_implicit", "kc_get_harvest", "kc_mlp_train",
               "kc_mlp_forward", "kc_mlp_grad", "kc_fp64_peak", "kc_set_graph", "kc_autotune",
               "kc_kdmp_write_header", "kc_kdmp_parse_header", "kc_kdmp_write", "kc_kdmp_load", "kc_kdmp_write_file",
-              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct", "kc_set_face_tiles",
+              "kc_kdmp_load_file", "kc_debug_fail_allocs", "kc_flux_ct", "kc_set_face_tiles", "kc_set_implicit_threads",
               "kc_set_harvest_filter"]:
         getattr(L, n).restype = ctypes.c_int
     _lib = L
@@ -314,6 +315,12 @@ class Sim:
     def set_graph(self, on):
         """Capture the step as a CUDA graph and replay it (bit-identical)."""
         self._check(self._lib.kc_set_graph(self._h, 1 if on else 0))
+
+    def set_implicit_threads(self, threads):
+        """Threads per block of the per-cell implicit kernel: 256, 384 (default)
+        or 512; one block fills an SM, so this sets its register budget (all
+        sizes give the same bits)."""
+        self._check(self._lib.kc_set_implicit_threads(self._h, threads))
 
     def set_face_tiles(self, mode):
         """The y and z face sweeps' form: 0 per face, 1 reconstructed-face tiles,

@@ -347,3 +347,26 @@ def test_face_tile_forms_bitwise(tiles):
             gpu.step()
             orc.step()
         _assert_same_state(gpu, orc)
+
+
+@pytest.mark.parametrize("threads", [256, 512])
+def test_implicit_block_sizes_bitwise(threads):
+    """The per-cell implicit kernel's other SM-wide blocks (255 and 128
+    registers; the default 384 runs in every other test): the perturbed 3D
+    wedge and a 2D grid, CFL steps bit for bit with the oracle, with the step
+    eager and as a graph; an unknown size is rejected."""
+    kc = _kc()
+    for nx, ny, nz in ((24, 20, 8), (32, 30, 1)):
+        grid, opt = kc.puffy_grid(nx, ny, nz), kc.puffy_options()
+        gpu, orc = _pair(grid, opt)
+        gpu.set_implicit_threads(threads)
+        with pytest.raises(kc.KoralError):
+            gpu.set_implicit_threads(128)
+        assert gpu.initPuffy(1e-3, 1e-3, 78) == orc.init_puffy(1e-3, 1e-3, 78)
+        orc.lib.orc_sim_init_timestep_guess(orc.h)
+        for k in range(4):
+            if k == 2:
+                gpu.set_graph(True)
+            gpu.step()
+            orc.step()
+        _assert_same_state(gpu, orc)
